@@ -1,0 +1,341 @@
+#!/usr/bin/env python3
+"""Benchmark of the single-GPU transform path: the 3D periodic Poisson solve at
+256^3 float32 (R2C, multiply by -1/|k|^2 with k = 0 zeroed, C2R, 1/N).
+
+One step = one R2C + C2R round trip over one 256^3 field (the fused Poisson
+solve).  The metric is algorithmic HBM GB/s: bytes = 2 * (4 N + 8 N_c) per
+round trip (N = 256^3 real points, N_c = 256*256*129 half-spectrum points), the
+bytes a round trip must read and write once.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fftb|reference]
+
+Device timing uses CUDA events on the launching stream.  Between timed steps a
+1 GiB buffer (larger than the 126 MB L2) is overwritten outside the timed
+window, so every step starts with a cold L2.  With N > 1 (torchrun), every rank
+solves its own field (replicas; the single transform does not shard) and the
+slowest rank's time is reported.  ``--impl reference`` times the CPU reference
+arm: the reference's CUDA path cannot be built here (its SCFD submodule is
+absent and its FFTs are cuFFT), so the arm runs the FP64 CPU restatement of
+its algorithm (oracle/) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "R2C+C2R ms & HBM GB/s at 256^3/64^4; TC/batched vs plain FP32 at err<=5e-6"
+NX = NY = NZ = 256
+N_REAL = NX * NY * NZ
+N_CPLX = NX * NY * (NZ // 2 + 1)
+BYTES_RT = 2 * (4 * N_REAL + 8 * N_CPLX)   # 269,484,032
+WORKLOAD = "3D periodic Poisson solve 256^3 f32: R2C, x(-1/|k|^2) (k=0 -> 0), C2R, 1/N"
+DATA = ("synthetic: f = sin x sin 2y cos 3z + 0.1*U[-1,1] (numpy default_rng(0)), mean removed, "
+        "grid x_i = 2 pi i / 256")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="fftb", choices=["fftb", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_rhs(dtype=np.float32):
+    g = 2 * np.pi * np.arange(NX) / NX
+    x = g[:, None, None]
+    y = g[None, :, None]
+    z = g[None, None, :]
+    f = np.sin(x) * np.sin(2 * y) * np.cos(3 * z)
+    rng = np.random.default_rng(0)
+    f = f + 0.1 * rng.uniform(-1.0, 1.0, (NX, NY, NZ))
+    f -= f.mean()
+    return np.ascontiguousarray(f.astype(dtype))
+
+
+# ---------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [v.strip() for v in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_name):
+    """DRAM bytes per launch of a kernel from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        v = d.get(kernel_name)
+        return None if v is None else float(v["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------- CPU legs
+def cpu_oracle_rate(f_host, sample_solves=1):
+    """FP64 oracle Poisson solve on all host threads; returns (GB/s, seconds, threads, solution)."""
+    import oracle as O
+    threads = O.max_threads()
+    O.set_threads(threads)
+    f64 = f_host.astype(np.float64)
+    t0 = time.perf_counter()
+    sol = None
+    for _ in range(sample_solves):
+        sol = O.poisson3d_solve(f64, -1.0)
+    dt = time.perf_counter() - t0
+    return BYTES_RT * sample_solves / dt / 1e9, dt, threads, sol
+
+
+def run_reference(args, rank):
+    """CPU reference arm (rank 0 only)."""
+    if rank != 0:
+        return
+    f = make_rhs(np.float32)
+    import oracle as O
+    threads = O.max_threads()
+    O.set_threads(threads)
+    f64 = f.astype(np.float64)
+    for _ in range(max(0, min(args.warmup, 1))):
+        O.poisson3d_solve(f64, -1.0)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.poisson3d_solve(f64, -1.0)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = BYTES_RT * args.steps / tot / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": DATA, "config": {"workload": WORKLOAD, "n": [NX, NY, NZ], "bytes_per_step": BYTES_RT},
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": "full 256^3 FP64 Poisson solve per step (oracle/fft_oracle.c, OpenMP)"},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": ("reference CUDA path not buildable here (SCFD submodule empty, cuFFT-only FFTs); "
+                 "arm = FP64 CPU restatement of its transform path"),
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------- GPU arm
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return 0
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from fftm_b200 import build as _build
+    if rank == 0 or world == 1:
+        _build.build()
+    if dist is not None:
+        dist.barrier()
+    import fftm_b200 as F
+
+    dev = torch.device("cuda", local)
+    f_host = make_rhs(np.float32)
+    rhs = torch.from_numpy(f_host).to(dev)
+    sol = torch.empty_like(rhs)
+    ff = F.ffts("float32").init(NX, NY, NZ)
+    work = torch.empty(ff.work_size // 8 + 1, dtype=torch.complex64, device=dev)
+    ff.set_work_area(work)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.float32, device=dev)   # 1 GiB > L2
+    stream = torch.cuda.current_stream()
+
+    def step():
+        ff.poisson(rhs, sol, -1.0)
+
+    for _ in range(max(3, args.warmup)):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+
+    launches_per_step = ff.num_launches("poisson")
+    ff.timing_enable(launches_per_step * args.steps + 8)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        flush.zero_()                # outside the timed window; also covers host enqueue time
+        starts[i].record(stream)
+        step()
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    per_launch = ff.timing_read()
+    ff.timing_enable(0)
+    if dist is not None:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = BYTES_RT * args.steps * world / (total_ms * 1e-3) / 1e9
+
+    # per-kernel roofline from the live per-launch events
+    agg = {}
+    for name, ms, by in per_launch:
+        a = agg.setdefault(name, [0, 0.0, by])
+        a[0] += 1
+        a[1] += ms
+    dom = max(agg.items(), key=lambda kv: kv[1][1])
+    dom_name, (dom_n, dom_ms, dom_bytes) = dom
+    peak, peak_kind = measured_hbm_peak()
+    avg_ms = dom_ms / dom_n
+    achieved = dom_bytes / (avg_ms * 1e-3) / 1e9
+    traffic = ncu_traffic(dom_name)
+    kernels = {k: {"launches": v[0], "avg_us": v[1] / v[0] * 1e3, "share": v[1] / max(1e-9, sum(x[1] for x in
+                                                                                                agg.values())),
+                   "alg_bytes": v[2], "gbs": v[2] / (v[1] / v[0] * 1e-3) / 1e9} for k, v in agg.items()}
+
+    # end to end through the public API with host buffers (pinned), copies inside the timed region
+    h_in = torch.from_numpy(f_host).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    d_in = torch.empty_like(rhs)
+    d_out = torch.empty_like(rhs)
+    e2e_steps = max(3, min(args.steps, 20))
+    for _ in range(2):
+        d_in.copy_(h_in, non_blocking=True)
+        ff.poisson(d_in, d_out, -1.0)
+        h_out.copy_(d_out, non_blocking=True)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        d_in.copy_(h_in, non_blocking=True)
+        ff.poisson(d_in, d_out, -1.0)
+        h_out.copy_(d_out, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_val = BYTES_RT * e2e_steps * world / (e2e_ms * 1e-3) / 1e9
+
+    # accuracy of the timed solution against the analytic solution of the smooth part is not
+    # defined (the noise term has no closed form); the CPU leg checks it against the FP64 oracle.
+    result = sol.detach().cpu().numpy()
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": DATA,
+        "config": {"workload": WORKLOAD, "n": [NX, NY, NZ], "bytes_per_step": BYTES_RT,
+                   "l2": "flushed between steps (1 GiB write outside the timed window)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "gpu_launches": launches_per_step * args.steps,
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic},
+        "kernels": kernels,
+        "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": int(rhs.numel() * 4),
+                "d2h_bytes_per_step": int(sol.numel() * 4), "steps": e2e_steps,
+                "ms_per_step": e2e_ms / e2e_steps},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, secs, threads, ref = cpu_oracle_rate(f_host, 1)
+        num = np.linalg.norm((result.astype(np.float64) - ref).ravel())
+        line["cpu_baseline"] = {"value": rate, "unit": "GB/s", "cores": threads, "kind": "port",
+                                "sample": "one full 256^3 FP64 Poisson solve (oracle/fft_oracle.c, OpenMP)",
+                                "seconds": secs}
+        line["accuracy"] = {"rel_l2_vs_fp64_oracle": float(num / np.linalg.norm(ref.ravel()))}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,83 @@
+"""ctypes binding of ``libfftb_b200.so`` (the C ABI declared in include/fftb.h).
+
+There is no fallback: if the shared library is missing or fails to load, every
+entry point raises.  Build it with ``python -m fftm_b200.build``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfftb_b200.so")
+
+# every symbol include/fftb.h declares (checked by the CPU tests)
+EXPORTS = [
+    "fftb_status_string", "fftb_last_error_message", "fftb_version",
+    "fftb_plan_create", "fftb_plan_get_work_size", "fftb_plan_set_work_area", "fftb_plan_set_stream",
+    "fftb_exec", "fftb_exec_direction", "fftb_plan_describe", "fftb_plan_num_launches", "fftb_plan_destroy",
+    "fftb_ffts_create", "fftb_ffts_destroy", "fftb_ffts_dimension", "fftb_ffts_work_size",
+    "fftb_ffts_set_work_area", "fftb_ffts_set_stream", "fftb_ffts_forward", "fftb_ffts_backward",
+    "fftb_ffts_backward_normalized", "fftb_ffts_poisson", "fftb_ffts_filter", "fftb_ffts_spectrum_poisson",
+    "fftb_ffts_num_launches", "fftb_ffts_timing_enable", "fftb_ffts_timing_read",
+]
+
+_lib = None
+
+
+def load():
+    """Loads the library (once) and declares the argument types."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"fftb CUDA library not built: {LIB_PATH} is missing "
+                          "(run `python -m fftm_b200.build`)")
+    L = ctypes.CDLL(LIB_PATH)
+    c_int, c_ll, c_vp, c_sz, c_d = ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_double
+    llp = ctypes.POINTER(c_ll)
+    ip = ctypes.POINTER(c_int)
+    szp = ctypes.POINTER(c_sz)
+    L.fftb_status_string.argtypes = [c_int]
+    L.fftb_status_string.restype = ctypes.c_char_p
+    L.fftb_version.restype = ctypes.c_char_p
+    L.fftb_last_error_message.restype = ctypes.c_char_p
+    L.fftb_plan_create.argtypes = [c_int, c_int, c_int, llp, llp, c_ll, c_ll, llp, c_ll, c_ll, c_ll,
+                                   ctypes.POINTER(c_vp), szp]
+    L.fftb_plan_get_work_size.argtypes = [c_vp, szp]
+    L.fftb_plan_set_work_area.argtypes = [c_vp, c_vp]
+    L.fftb_plan_set_stream.argtypes = [c_vp, c_vp]
+    L.fftb_exec.argtypes = [c_vp, c_vp, c_vp]
+    L.fftb_exec_direction.argtypes = [c_vp, c_int, c_vp, c_vp]
+    L.fftb_plan_describe.argtypes = [c_vp, ip, ip, ip, llp, llp, llp, llp, llp, llp, llp, llp]
+    L.fftb_plan_num_launches.argtypes = [c_vp, ip]
+    L.fftb_plan_destroy.argtypes = [c_vp]
+    L.fftb_ffts_create.argtypes = [c_int, c_ll, c_ll, c_ll, c_ll, c_int, ctypes.POINTER(c_vp)]
+    L.fftb_ffts_destroy.argtypes = [c_vp]
+    L.fftb_ffts_dimension.argtypes = [c_vp, ip]
+    L.fftb_ffts_work_size.argtypes = [c_vp, szp]
+    L.fftb_ffts_set_work_area.argtypes = [c_vp, c_vp]
+    L.fftb_ffts_set_stream.argtypes = [c_vp, c_vp]
+    L.fftb_ffts_forward.argtypes = [c_vp, c_vp, c_vp]
+    L.fftb_ffts_backward.argtypes = [c_vp, c_vp, c_vp]
+    L.fftb_ffts_backward_normalized.argtypes = [c_vp, c_vp, c_vp]
+    L.fftb_ffts_poisson.argtypes = [c_vp, c_vp, c_vp, c_d]
+    L.fftb_ffts_filter.argtypes = [c_vp, c_vp, c_vp, c_d, c_d]
+    L.fftb_ffts_spectrum_poisson.argtypes = [c_vp, c_vp, c_d, c_d]
+    L.fftb_ffts_num_launches.argtypes = [c_vp, c_int, ip]
+    L.fftb_ffts_timing_enable.argtypes = [c_vp, c_int]
+    L.fftb_ffts_timing_read.argtypes = [c_vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(c_d),
+                                        ctypes.c_char_p, c_int, c_int, ip]
+    for name in EXPORTS:
+        if name not in ("fftb_status_string", "fftb_version", "fftb_last_error_message"):
+            getattr(L, name).restype = c_int
+    _lib = L
+    return L
+
+
+def status_string(st: int) -> str:
+    return load().fftb_status_string(int(st)).decode()
+
+
+def last_error_message() -> str:
+    return load().fftb_last_error_message().decode()

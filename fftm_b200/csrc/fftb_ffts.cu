@@ -1,0 +1,539 @@
+// fftb_ffts.cu -- the `ffts` transform objects (replacement for fftm::ffts,
+// reference source/ffts.hpp:159-383) on the pass engine.
+//
+// Every stage of the reference pipeline (cuFFT plan + SCFD transpose functor)
+// becomes one pass of the engine whose load/store geometry absorbs the
+// transpose; the Poisson / filter multiply becomes the epilogue of a
+// forward-multiply-inverse "sandwich" pass on the last axis, and the 1/N scale
+// the epilogue of the final C2R pass.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+
+#include "../../include/fftb.h"
+#include "fftb_device.cuh"
+#include "fftb_engine.h"
+#include "fftb_fused3d.h"
+
+using namespace fftb;
+
+struct fftb_ffts_s {
+    int dtype = 0, dim = 0, layout = 0;
+    long long nx = 0, ny = 0, nz = 0, nw = 0;
+    Program fwd, bwd, bwd_norm, poisson, filter;
+    size_t work_bytes = 0;
+    void *work = nullptr;
+    bool own_work = false;
+    cudaStream_t stream = 0;
+    Fused3D fused;  // specialised 3D kernels (when the size has them)
+    LaunchTimer timer;
+    bool timing = false;
+};
+
+namespace {
+
+AxisPass mkpass(int kind, long long n, long long is, long long os, std::vector<Dim> batch, int in_buf, int out_buf)
+{
+    AxisPass p;
+    p.kind = kind;
+    p.n = (int)n;
+    p.is = is;
+    p.os = os;
+    p.batch = std::move(batch);
+    p.in_buf = in_buf;
+    p.out_buf = out_buf;
+    return p;
+}
+
+AxisPass with_scale(AxisPass p, double s)
+{
+    p.ep_mode |= EP_SCALE;
+    p.ep_scale = s;
+    return p;
+}
+
+AxisPass sandwich(AxisPass p, std::vector<EpAxis> axes)
+{
+    p.kind = K_SANDWICH;
+    p.ep_mode = EP_SCALE | EP_POISSON;
+    p.ep_axes = std::move(axes);
+    p.ep_dynamic = 1;
+    return p;
+}
+
+#define TRY(x)                                                                                                        \
+    do {                                                                                                              \
+        int _s = (x);                                                                                                 \
+        if (_s != FFTB_SUCCESS) return _s;                                                                            \
+    } while (0)
+
+int build_2d(fftb_ffts_s *o)
+{
+    const long long nx = o->nx, ny = o->ny, nyh = ny / 2 + 1;
+    const double invN = 1.0 / (double)(nx * ny);
+    const int d = o->dtype;
+    AxisPass r2c = mkpass(K_R2C, ny, 1, 1, {Dim{nx, ny, nyh, 0}}, B_IN, B_OUT);
+    AxisPass xf = mkpass(K_C2C_FWD, nx, nyh, nyh, {Dim{nyh, 1, 1, 1}}, B_OUT, B_OUT);
+    TRY(program_add(o->fwd, d, r2c));
+    TRY(program_add(o->fwd, d, xf));
+    AxisPass xi = mkpass(K_C2C_INV, nx, nyh, nyh, {Dim{nyh, 1, 1, 1}}, B_IN, B_IN);
+    AxisPass c2r = mkpass(K_C2R, ny, 1, 1, {Dim{nx, nyh, ny, 0}}, B_IN, B_OUT);
+    TRY(program_add(o->bwd, d, xi));
+    TRY(program_add(o->bwd, d, c2r));
+    TRY(program_add(o->bwd_norm, d, xi));
+    TRY(program_add(o->bwd_norm, d, with_scale(c2r, invN)));
+    for (int f = 0; f < 2; ++f) {
+        Program &pr = f ? o->filter : o->poisson;
+        AxisPass a = r2c;
+        a.out_buf = B_WORK;
+        AxisPass s = xf;
+        s.in_buf = s.out_buf = B_WORK;
+        s = sandwich(s, {EpAxis{1, -1, (int)nx, 0}, EpAxis{0, 1, (int)ny, 1}});
+        AxisPass c = with_scale(c2r, invN);
+        c.in_buf = B_WORK;
+        TRY(program_add(pr, d, a));
+        TRY(program_add(pr, d, s));
+        TRY(program_add(pr, d, c));
+    }
+    o->work_bytes = complex_bytes(d) * (size_t)(nx * nyh);
+    return FFTB_SUCCESS;
+}
+
+int build_3d(fftb_ffts_s *o)
+{
+    const long long nx = o->nx, ny = o->ny, nz = o->nz, nzh = nz / 2 + 1, C3 = ny * nzh;
+    const double invN = 1.0 / (double)(nx * ny * nz);
+    const int d = o->dtype;
+    // forward_3d: source/ffts.hpp:680-686
+    AxisPass zr = mkpass(K_R2C, nz, 1, 1, {Dim{ny, nz, nzh, 1}, Dim{nx, ny * nz, C3, 0}}, B_IN, B_OUT);
+    AxisPass yf = mkpass(K_C2C_FWD, ny, nzh, nzh, {Dim{nzh, 1, 1, 2}, Dim{nx, C3, C3, 0}}, B_OUT, B_OUT);
+    AxisPass xf = mkpass(K_C2C_FWD, nx, C3, C3, {Dim{nzh, 1, 1, 2}, Dim{ny, nzh, nzh, 1}}, B_OUT, B_OUT);
+    TRY(program_add(o->fwd, d, zr));
+    TRY(program_add(o->fwd, d, yf));
+    TRY(program_add(o->fwd, d, xf));
+    // inverse_3d: source/ffts.hpp:688-694 (destructive on the spectrum, like cuFFT C2R)
+    AxisPass xi = mkpass(K_C2C_INV, nx, C3, C3, {Dim{nzh, 1, 1, 2}, Dim{ny, nzh, nzh, 1}}, B_IN, B_IN);
+    AxisPass yi = mkpass(K_C2C_INV, ny, nzh, nzh, {Dim{nzh, 1, 1, 2}, Dim{nx, C3, C3, 0}}, B_IN, B_IN);
+    AxisPass zc = mkpass(K_C2R, nz, 1, 1, {Dim{ny, nzh, nz, 1}, Dim{nx, C3, ny * nz, 0}}, B_IN, B_OUT);
+    TRY(program_add(o->bwd, d, xi));
+    TRY(program_add(o->bwd, d, yi));
+    TRY(program_add(o->bwd, d, zc));
+    TRY(program_add(o->bwd_norm, d, xi));
+    TRY(program_add(o->bwd_norm, d, yi));
+    TRY(program_add(o->bwd_norm, d, with_scale(zc, invN)));
+    for (int f = 0; f < 2; ++f) {
+        Program &pr = f ? o->filter : o->poisson;
+        AxisPass a = zr;
+        a.out_buf = B_WORK;
+        AxisPass y1 = yf;
+        y1.in_buf = y1.out_buf = B_WORK;
+        AxisPass s = xf;
+        s.in_buf = s.out_buf = B_WORK;
+        s = sandwich(s, {EpAxis{1, -1, (int)nx, 0}, EpAxis{0, 1, (int)ny, 0}, EpAxis{0, 2, (int)nz, 1}});
+        AxisPass y2 = yi;
+        y2.in_buf = y2.out_buf = B_WORK;
+        AxisPass c = with_scale(zc, invN);
+        c.in_buf = B_WORK;
+        TRY(program_add(pr, d, a));
+        TRY(program_add(pr, d, y1));
+        TRY(program_add(pr, d, s));
+        TRY(program_add(pr, d, y2));
+        TRY(program_add(pr, d, c));
+    }
+    o->work_bytes = complex_bytes(d) * (size_t)(nx * C3);
+    return FFTB_SUCCESS;
+}
+
+int build_4d(fftb_ffts_s *o)
+{
+    const long long nx = o->nx, ny = o->ny, nz = o->nz, nw = o->nw, nwh = nw / 2 + 1;
+    const double invN = 1.0 / (double)(nx * ny * nz * nw);
+    const int d = o->dtype;
+    o->work_bytes = complex_bytes(d) * (size_t)(nx * ny * nz * nwh);
+    if (o->layout == FFTB_4D_SLAB || o->layout == FFTB_4D_NATIVE_XZWY) {
+        const long long C = nz * nwh;
+        // slab stage 0: 2D R2C over (z,w) per (x,y) (source/ffts.hpp:751-763), split into w then z
+        AxisPass wr = mkpass(K_R2C, nw, 1, 1,
+                             {Dim{nz, nw, nwh, 2}, Dim{ny, nz * nw, C, 1}, Dim{nx, ny * nz * nw, ny * C, 0}}, B_IN,
+                             B_OUT);
+        AxisPass zf = mkpass(K_C2C_FWD, nz, nwh, nwh, {Dim{nwh, 1, 1, 3}, Dim{ny, C, C, 1}, Dim{nx, ny * C, ny * C, 0}},
+                             B_OUT, B_OUT);
+        AxisPass yf = mkpass(K_C2C_FWD, ny, C, C, {Dim{nwh, 1, 1, 3}, Dim{nz, nwh, nwh, 2}, Dim{nx, ny * C, ny * C, 0}},
+                             B_OUT, B_OUT);
+        AxisPass xf = mkpass(K_C2C_FWD, nx, ny * C, ny * C, {Dim{nwh, 1, 1, 3}, Dim{nz, nwh, nwh, 2}, Dim{ny, C, C, 1}},
+                             B_OUT, B_OUT);
+        AxisPass wc = mkpass(K_C2R, nw, 1, 1,
+                             {Dim{nz, nwh, nw, 2}, Dim{ny, C, nz * nw, 1}, Dim{nx, ny * C, ny * nz * nw, 0}}, B_IN,
+                             B_OUT);
+        auto on = [](AxisPass p, int ib, int ob) { p.in_buf = ib; p.out_buf = ob; return p; };
+        auto inv = [](AxisPass p) { p.kind = K_C2C_INV; return p; };
+        if (o->layout == FFTB_4D_SLAB) {
+            TRY(program_add(o->fwd, d, wr));
+            TRY(program_add(o->fwd, d, zf));
+            TRY(program_add(o->fwd, d, yf));
+            TRY(program_add(o->fwd, d, xf));
+            for (int nrm = 0; nrm < 2; ++nrm) {
+                Program &pr = nrm ? o->bwd_norm : o->bwd;
+                TRY(program_add(pr, d, on(inv(xf), B_IN, B_IN)));
+                TRY(program_add(pr, d, on(inv(yf), B_IN, B_IN)));
+                TRY(program_add(pr, d, on(inv(zf), B_IN, B_IN)));
+                TRY(program_add(pr, d, nrm ? with_scale(wc, invN) : wc));
+            }
+        } else {
+            // native_xzwy: the (y,x) C2C of source/fftm.hpp:2941-2961 with the local permute to
+            // [ky][kz][kw][kx] fused into the x pass
+            TRY(program_add(o->fwd, d, on(wr, B_IN, B_WORK)));
+            TRY(program_add(o->fwd, d, on(zf, B_WORK, B_WORK)));
+            TRY(program_add(o->fwd, d, on(yf, B_WORK, B_WORK)));
+            AxisPass xp = mkpass(K_C2C_FWD, nx, ny * C, 1,
+                                 {Dim{nwh, 1, nx, 3}, Dim{nz, nwh, nwh * nx, 2}, Dim{ny, C, C * nx, 1}}, B_WORK, B_OUT);
+            TRY(program_add(o->fwd, d, xp));
+            AxisPass xq = mkpass(K_C2C_INV, nx, 1, ny * C,
+                                 {Dim{nwh, nx, 1, 3}, Dim{nz, nwh * nx, nwh, 2}, Dim{ny, C * nx, C, 1}}, B_IN, B_WORK);
+            for (int nrm = 0; nrm < 2; ++nrm) {
+                Program &pr = nrm ? o->bwd_norm : o->bwd;
+                TRY(program_add(pr, d, xq));
+                TRY(program_add(pr, d, on(inv(yf), B_WORK, B_WORK)));
+                TRY(program_add(pr, d, on(inv(zf), B_WORK, B_WORK)));
+                TRY(program_add(pr, d, on(nrm ? with_scale(wc, invN) : wc, B_WORK, B_OUT)));
+            }
+        }
+        for (int f = 0; f < 2; ++f) {
+            Program &pr = f ? o->filter : o->poisson;
+            TRY(program_add(pr, d, on(wr, B_IN, B_WORK)));
+            TRY(program_add(pr, d, on(zf, B_WORK, B_WORK)));
+            TRY(program_add(pr, d, on(yf, B_WORK, B_WORK)));
+            TRY(program_add(pr, d, sandwich(on(xf, B_WORK, B_WORK),
+                                            {EpAxis{1, -1, (int)nx, 0}, EpAxis{0, 1, (int)ny, 0},
+                                             EpAxis{0, 2, (int)nz, 0}, EpAxis{0, 3, (int)nw, 1}})));
+            TRY(program_add(pr, d, on(inv(yf), B_WORK, B_WORK)));
+            TRY(program_add(pr, d, on(inv(zf), B_WORK, B_WORK)));
+            TRY(program_add(pr, d, on(with_scale(wc, invN), B_WORK, B_OUT)));
+        }
+    } else if (o->layout == FFTB_4D_PENCIL) {
+        const long long Vs = nx * ny * nz;
+        // forward_w .. forward_x with the three transposes of source/ffts.hpp:809-825 fused
+        AxisPass wr = mkpass(K_R2C, nw, Vs, Vs, {Dim{nx, 1, 1, 0}, Dim{ny, nx, nx, 1}, Dim{nz, nx * ny, nx * ny, 2}},
+                             B_IN, B_WORK);
+        AxisPass zf = mkpass(K_C2C_FWD, nz, nx * ny, nx * ny,
+                             {Dim{nx, 1, 1, 0}, Dim{ny, nx, nx, 1}, Dim{nwh, Vs, Vs, 3}}, B_WORK, B_WORK);
+        AxisPass yf = mkpass(K_C2C_FWD, ny, nx, nx,
+                             {Dim{nx, 1, 1, 0}, Dim{nz, nx * ny, nx * ny, 2}, Dim{nwh, Vs, Vs, 3}}, B_WORK, B_WORK);
+        AxisPass xp = mkpass(K_C2C_FWD, nx, 1, 1,
+                             {Dim{ny, nx, nz * nwh * nx, 1}, Dim{nz, nx * ny, nwh * nx, 2}, Dim{nwh, Vs, nx, 3}},
+                             B_WORK, B_OUT);
+        AxisPass xq = mkpass(K_C2C_INV, nx, 1, 1,
+                             {Dim{ny, nz * nwh * nx, nx, 1}, Dim{nz, nwh * nx, nx * ny, 2}, Dim{nwh, nx, Vs, 3}},
+                             B_IN, B_WORK);
+        AxisPass wc = mkpass(K_C2R, nw, Vs, Vs, {Dim{nx, 1, 1, 0}, Dim{ny, nx, nx, 1}, Dim{nz, nx * ny, nx * ny, 2}},
+                             B_WORK, B_OUT);
+        auto inv = [](AxisPass p) { p.kind = K_C2C_INV; return p; };
+        TRY(program_add(o->fwd, d, wr));
+        TRY(program_add(o->fwd, d, zf));
+        TRY(program_add(o->fwd, d, yf));
+        TRY(program_add(o->fwd, d, xp));
+        for (int nrm = 0; nrm < 2; ++nrm) {
+            Program &pr = nrm ? o->bwd_norm : o->bwd;
+            TRY(program_add(pr, d, xq));
+            TRY(program_add(pr, d, inv(yf)));
+            TRY(program_add(pr, d, inv(zf)));
+            TRY(program_add(pr, d, nrm ? with_scale(wc, invN) : wc));
+        }
+        AxisPass xs = mkpass(K_C2C_FWD, nx, 1, 1, {Dim{ny, nx, nx, 1}, Dim{nz, nx * ny, nx * ny, 2}, Dim{nwh, Vs, Vs, 3}},
+                             B_WORK, B_WORK);
+        for (int f = 0; f < 2; ++f) {
+            Program &pr = f ? o->filter : o->poisson;
+            TRY(program_add(pr, d, wr));
+            TRY(program_add(pr, d, zf));
+            TRY(program_add(pr, d, yf));
+            TRY(program_add(pr, d, sandwich(xs, {EpAxis{1, -1, (int)nx, 0}, EpAxis{0, 1, (int)ny, 0},
+                                                 EpAxis{0, 2, (int)nz, 0}, EpAxis{0, 3, (int)nw, 1}})));
+            TRY(program_add(pr, d, inv(yf)));
+            TRY(program_add(pr, d, inv(zf)));
+            TRY(program_add(pr, d, with_scale(wc, invN)));
+        }
+    } else {
+        return FFTB_ERROR_INVALID_VALUE;
+    }
+    return FFTB_SUCCESS;
+}
+
+int ensure_work(fftb_ffts_s *o)
+{
+    if (o->work || o->work_bytes == 0) return FFTB_SUCCESS;
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, o->work_bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return FFTB_ERROR_ALLOC;
+    }
+    o->work = p;
+    o->own_work = true;
+    return FFTB_SUCCESS;
+}
+
+bool needs_work(const Program &p)
+{
+    for (const Launch &L : p.launches)
+        if (L.in_buf == B_WORK || L.out_buf == B_WORK) return true;
+    return false;
+}
+
+int run(fftb_ffts_s *o, const Program &p, const void *in, void *out, const EpValues *ep)
+{
+    if (needs_work(p)) {
+        int st = ensure_work(o);
+        if (st != FFTB_SUCCESS) return st;
+    }
+    return program_exec(p, const_cast<void *>(in), out, o->work, o->stream, ep, o->timing ? &o->timer : nullptr);
+}
+
+// ---------------------------------------------------------------- standalone spectral multiply
+template <typename R>
+__global__ void spectrum_poisson_kernel(cpx<R> *s, long long total, int4 dims, int4 ns, int half_axis, R sign,
+                                        R scale)
+{
+    const int d[4] = {dims.x, dims.y, dims.z, dims.w};
+    const int n[4] = {ns.x, ns.y, ns.z, ns.w};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long r = i;
+        R k2 = R(0);
+#pragma unroll
+        for (int a = 3; a >= 0; --a) {
+            const int idx = (int)(r % d[a]);
+            r /= d[a];
+            const int k = (a == half_axis) ? idx : (idx <= n[a] / 2 ? idx : idx - n[a]);
+            k2 += R(k) * R(k);
+        }
+        cpx<R> v = s[i];
+        const R f = (k2 == R(0)) ? R(0) : scale * sign / k2;
+        v.x *= f;
+        v.y *= f;
+        s[i] = v;
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+int fftb_ffts_create(int dtype, long long nx, long long ny, long long nz, long long nw, int layout4d, fftb_ffts *obj)
+{
+    if (!obj) return FFTB_ERROR_INVALID_VALUE;
+    *obj = nullptr;
+    if (dtype != FFTB_F32 && dtype != FFTB_F64) return FFTB_ERROR_INVALID_VALUE;
+    if (nx < 1 || ny < 1 || nz < 0 || nw < 0 || (nz == 0 && nw > 0)) return FFTB_ERROR_INVALID_VALUE;
+    fftb_ffts_s *o = new (std::nothrow) fftb_ffts_s();
+    if (!o) return FFTB_ERROR_ALLOC;
+    o->dtype = dtype;
+    o->nx = nx;
+    o->ny = ny;
+    o->nz = nz;
+    o->nw = nw;
+    o->layout = layout4d;
+    o->dim = nz == 0 ? 2 : (nw == 0 ? 3 : 4);
+    int st;
+    if (o->dim == 2) st = build_2d(o);
+    else if (o->dim == 3) st = build_3d(o);
+    else st = build_4d(o);
+    if (st == FFTB_SUCCESS && o->dim == 3) st = fused3d_init(o->fused, dtype, nx, ny, nz);
+    if (st != FFTB_SUCCESS) {
+        delete o;
+        return st;
+    }
+    *obj = o;
+    return FFTB_SUCCESS;
+}
+
+int fftb_ffts_destroy(fftb_ffts o)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (o->own_work && o->work) cudaFree(o->work);
+    delete o;
+    return FFTB_SUCCESS;
+}
+
+int fftb_ffts_dimension(fftb_ffts o, int *dim)
+{
+    if (!o || !dim) return FFTB_ERROR_INVALID_HANDLE;
+    *dim = o->dim;
+    return FFTB_SUCCESS;
+}
+
+int fftb_ffts_work_size(fftb_ffts o, size_t *bytes)
+{
+    if (!o || !bytes) return FFTB_ERROR_INVALID_HANDLE;
+    *bytes = o->work_bytes;
+    return FFTB_SUCCESS;
+}
+
+int fftb_ffts_set_work_area(fftb_ffts o, void *work)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if ((uintptr_t)work % 256 != 0) return FFTB_ERROR_MISALIGNED;
+    if (o->own_work && o->work) cudaFree(o->work);
+    o->own_work = false;
+    o->work = work;
+    return FFTB_SUCCESS;
+}
+
+int fftb_ffts_set_stream(fftb_ffts o, void *stream)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    o->stream = (cudaStream_t)stream;
+    return FFTB_SUCCESS;
+}
+
+int fftb_ffts_forward(fftb_ffts o, const void *in, void *out)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (!in || !out) return FFTB_ERROR_INVALID_VALUE;
+    if (o->fused.enabled) return fused3d_forward(o->fused, in, out, o->stream, o->timing ? &o->timer : nullptr);
+    return run(o, o->fwd, in, out, nullptr);
+}
+
+int fftb_ffts_backward(fftb_ffts o, void *in, void *out)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (!in || !out) return FFTB_ERROR_INVALID_VALUE;
+    if (o->fused.enabled) return fused3d_backward(o->fused, in, out, 1.0, o->stream, o->timing ? &o->timer : nullptr);
+    return run(o, o->bwd, in, out, nullptr);
+}
+
+int fftb_ffts_backward_normalized(fftb_ffts o, void *in, void *out)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (!in || !out) return FFTB_ERROR_INVALID_VALUE;
+    if (o->fused.enabled)
+        return fused3d_backward(o->fused, in, out, 1.0 / (double)(o->nx * o->ny * o->nz), o->stream,
+                                o->timing ? &o->timer : nullptr);
+    return run(o, o->bwd_norm, in, out, nullptr);
+}
+
+int fftb_ffts_poisson(fftb_ffts o, const void *rhs, void *sol, double sign)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (!rhs || !sol) return FFTB_ERROR_INVALID_VALUE;
+    EpValues ep;
+    ep.scale = 1.0;
+    ep.sign = sign;
+    ep.mode = EP_SCALE | EP_POISSON;
+    if (o->fused.enabled) {
+        int st = ensure_work(o);
+        if (st != FFTB_SUCCESS) return st;
+        return fused3d_spectral(o->fused, rhs, sol, o->work, ep, o->stream, o->timing ? &o->timer : nullptr);
+    }
+    return run(o, o->poisson, rhs, sol, &ep);
+}
+
+int fftb_ffts_filter(fftb_ffts o, const void *in, void *out, double sigma, double poisson_sign)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (!in || !out || !(sigma > 0.0)) return FFTB_ERROR_INVALID_VALUE;
+    EpValues ep;
+    ep.scale = 1.0;
+    ep.sign = poisson_sign;
+    ep.gauss = 1.0 / (2.0 * sigma * sigma);
+    ep.mode = EP_SCALE | EP_GAUSS | (poisson_sign != 0.0 ? EP_POISSON : 0);
+    if (o->fused.enabled) {
+        int st = ensure_work(o);
+        if (st != FFTB_SUCCESS) return st;
+        return fused3d_spectral(o->fused, in, out, o->work, ep, o->stream, o->timing ? &o->timer : nullptr);
+    }
+    return run(o, o->filter, in, out, &ep);
+}
+
+int fftb_ffts_spectrum_poisson(fftb_ffts o, void *spec, double sign, double scale)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (!spec) return FFTB_ERROR_INVALID_VALUE;
+    int4 dims, ns;
+    int half_axis;
+    const int nxh = 0;
+    (void)nxh;
+    if (o->dim == 2) {
+        dims = make_int4(1, 1, (int)o->nx, (int)(o->ny / 2 + 1));
+        ns = make_int4(1, 1, (int)o->nx, (int)o->ny);
+        half_axis = 3;
+    } else if (o->dim == 3) {
+        dims = make_int4(1, (int)o->nx, (int)o->ny, (int)(o->nz / 2 + 1));
+        ns = make_int4(1, (int)o->nx, (int)o->ny, (int)o->nz);
+        half_axis = 3;
+    } else if (o->layout == FFTB_4D_SLAB) {
+        dims = make_int4((int)o->nx, (int)o->ny, (int)o->nz, (int)(o->nw / 2 + 1));
+        ns = make_int4((int)o->nx, (int)o->ny, (int)o->nz, (int)o->nw);
+        half_axis = 3;
+    } else {
+        dims = make_int4((int)o->ny, (int)o->nz, (int)(o->nw / 2 + 1), (int)o->nx);
+        ns = make_int4((int)o->ny, (int)o->nz, (int)o->nw, (int)o->nx);
+        half_axis = 2;
+    }
+    const long long total = (long long)dims.x * dims.y * dims.z * dims.w;
+    const int bs = 256;
+    const long long gs = std::min<long long>((total + bs - 1) / bs, 148LL * 16);
+    if (o->dtype == FFTB_F32)
+        spectrum_poisson_kernel<float><<<(unsigned)gs, bs, 0, o->stream>>>((float2 *)spec, total, dims, ns, half_axis,
+                                                                           (float)sign, (float)scale);
+    else
+        spectrum_poisson_kernel<double><<<(unsigned)gs, bs, 0, o->stream>>>((double2 *)spec, total, dims, ns,
+                                                                            half_axis, sign, scale);
+    return set_status_from_cuda(cudaGetLastError());
+}
+
+int fftb_ffts_timing_enable(fftb_ffts o, int max_launches)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (max_launches <= 0) {
+        o->timer.release();
+        o->timing = false;
+        return FFTB_SUCCESS;
+    }
+    int st = o->timer.reserve((size_t)max_launches * 2 + 2);
+    o->timing = (st == FFTB_SUCCESS);
+    return st;
+}
+
+int fftb_ffts_timing_read(fftb_ffts o, float *ms, double *bytes, char *names, int name_stride, int cap, int *count)
+{
+    if (!o || !count) return FFTB_ERROR_INVALID_HANDLE;
+    LaunchTimer &t = o->timer;
+    *count = 0;
+    if (t.used == 0) return FFTB_SUCCESS;
+    cudaError_t e = cudaEventSynchronize(t.ev[t.used - 1]);
+    if (e != cudaSuccess) return set_status_from_cuda(e);
+    int n = 0;
+    for (size_t i = 0; i + 1 < t.used; ++i) {
+        if (t.owner[i] != 1) continue;
+        if (n < cap) {
+            float v = 0.f;
+            e = cudaEventElapsedTime(&v, t.ev[i], t.ev[i + 1]);
+            if (e != cudaSuccess) return set_status_from_cuda(e);
+            if (ms) ms[n] = v;
+            if (bytes) bytes[n] = t.bytes[i];
+            if (names && name_stride > 0) {
+                strncpy(names + (size_t)n * name_stride, t.names[i].c_str(), (size_t)name_stride - 1);
+                names[(size_t)n * name_stride + name_stride - 1] = 0;
+            }
+        }
+        ++n;
+    }
+    *count = n < cap ? n : cap;
+    t.used = 0;
+    return FFTB_SUCCESS;
+}
+
+int fftb_ffts_num_launches(fftb_ffts o, int which, int *launches)
+{
+    if (!o || !launches) return FFTB_ERROR_INVALID_HANDLE;
+    if (o->fused.enabled) {
+        *launches = fused3d_num_launches(o->fused, which);
+        return FFTB_SUCCESS;
+    }
+    const Program *p = which == 0 ? &o->fwd : which == 1 ? &o->bwd : which == 2 ? &o->poisson : &o->filter;
+    *launches = (int)p->launches.size();
+    return FFTB_SUCCESS;
+}
+
+} // extern "C"

@@ -1,0 +1,26 @@
+// fftb_fused3d.h -- specialised 3D kernels (fused multi-axis passes) for the
+// sizes that have them; the generic pass programs cover every other size.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fftb_engine.h"
+
+namespace fftb {
+
+struct Fused3D {
+    bool enabled = false;
+    int dtype = 0;
+    long long nx = 0, ny = 0, nz = 0;
+    Program xfwd, xinv, xsand;  // generic x-axis passes used between the fused kernels
+};
+
+// Sets f.enabled when (dtype, nx, ny, nz) has a specialised path.
+int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz);
+int fused3d_forward(const Fused3D &f, const void *in, void *out, cudaStream_t s, LaunchTimer *t);
+int fused3d_backward(const Fused3D &f, void *in, void *out, double scale, cudaStream_t s, LaunchTimer *t);
+int fused3d_spectral(const Fused3D &f, const void *in, void *out, void *work, const EpValues &ep, cudaStream_t s,
+                     LaunchTimer *t);
+int fused3d_num_launches(const Fused3D &f, int which);
+
+} // namespace fftb

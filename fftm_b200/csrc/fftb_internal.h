@@ -1,0 +1,60 @@
+// fftb_internal.h -- host/device shared structures of the fftb engine.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace fftb {
+
+// pass kinds
+enum PassKind : int {
+    K_C2C_FWD = 0,
+    K_C2C_INV = 1,
+    K_R2C = 2,
+    K_C2R = 3,
+    K_SANDWICH = 4,  // forward FFT, spectral multiply, inverse FFT in one pass
+};
+
+// epilogue (spectral multiplier) flags
+enum EpMode : int {
+    EP_SCALE = 1,    // multiply by ep_scale
+    EP_POISSON = 2,  // multiply by ep_sign / |k|^2 (0 at k = 0)
+    EP_GAUSS = 4,    // multiply by exp(-|k|^2 * ep_gauss)
+};
+
+// Everything one pass launch needs.  POD, passed by value.
+struct PassArgs {
+    const void *in;
+    void *out;
+    long long is, os;         // stride between the points of a line (elements of the in/out type)
+    long long nlines;         // L
+    long long c0, c1;         // batch dims: b0 = l % c0, b1 = (l / c0) % c1, b2 = l / (c0*c1)
+    long long ib0, ib1, ib2;  // input offsets per batch index
+    long long ob0, ob1, ob2;  // output offsets per batch index
+    int kind;
+    int half;                 // R2C/C2R through the half-length complex packing (even length)
+    int in_pts_fast, out_pts_fast;
+    int pair_io;              // real side accessed as aligned (even, odd) pairs
+    int G, gshift;            // lines per CTA (power of two)
+    const void *tw;           // forward roots exp(-2 pi i m / ntw), m in [0, ntw)
+    int ntw;
+    int tw_smem;              // stage the root table in shared memory
+    // epilogue
+    int ep_mode;
+    int ep_naxes;
+    int ep_src[4];            // 0: point index, 1..3: batch index b0..b2
+    int ep_n[4];
+    int ep_half[4];
+    double ep_kscale[4];
+    double ep_scale, ep_sign, ep_gauss;
+};
+
+struct PassKernelInfo {
+    int nf;
+    int threads_per_line;
+    int line_pitch;
+    const void *fn;
+};
+
+} // namespace fftb

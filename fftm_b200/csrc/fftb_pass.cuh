@@ -1,0 +1,258 @@
+// fftb_pass.cuh -- the generic strided/batched 1D FFT pass kernel.
+//
+// One launch transforms L independent lines of one axis.  A CTA owns G
+// consecutive lines (G a power of two), stages them in shared memory with
+// coalesced loads (points-fastest when the axis is contiguous, lines-fastest when
+// the lines are), runs the Stockham core on each line with T threads, applies
+// the fused spectral epilogue and writes the lines back with coalesced stores.
+// Input and output geometries are independent, so a pass can also permute the
+// array (this is how the 4D layout changes of the reference's transposes,
+// source/detail/direct_transpose_4d.h:17-32, are fused into the FFT passes).
+#pragma once
+
+#include "fftb_device.cuh"
+#include "fftb_internal.h"
+
+namespace fftb {
+
+template <typename R> __device__ __forceinline__ R ep_factor(const PassArgs &a, int p, const int *bidx)
+{
+    R k2 = R(0);
+#pragma unroll 4
+    for (int ax = 0; ax < a.ep_naxes; ++ax) {
+        const int src = a.ep_src[ax];
+        const int i = src == 0 ? p : bidx[src - 1];
+        const int n = a.ep_n[ax];
+        const int k = a.ep_half[ax] ? i : (i <= n / 2 ? i : i - n);
+        const R kk = R(k) * R(a.ep_kscale[ax]);
+        k2 += kk * kk;
+    }
+    R f = R(a.ep_scale);
+    if (a.ep_mode & EP_POISSON) f = (k2 == R(0)) ? R(0) : f * R(a.ep_sign) / k2;
+    if (a.ep_mode & EP_GAUSS) f *= exp(-k2 * R(a.ep_gauss));
+    return f;
+}
+
+template <typename R, int NF>
+__global__ void __launch_bounds__(512) fftb_pass_kernel(PassArgs a)
+{
+    using C = cpx<R>;
+    constexpr int T = threads_per_line(NF);
+    constexpr int LP = pad16(NF) + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *stw_s = reinterpret_cast<C *>(smem_raw);
+    const int ntw_s = a.tw_smem ? a.ntw : 0;
+    long long *offs = reinterpret_cast<long long *>(stw_s + ntw_s);  // [G][2] in/out offsets
+    int *bidx = reinterpret_cast<int *>(offs + 2 * a.G);            // [G][3]
+    C *lines = reinterpret_cast<C *>(bidx + 4 * a.G);               // [G][LP]
+
+    const int tid = threadIdx.x;
+    const int G = a.G;
+    const int gshift = a.gshift;
+    const int g = tid / T;
+    const int t = tid - g * T;
+    const long long line0 = (long long)blockIdx.x * G;
+
+    const C *twg = reinterpret_cast<const C *>(a.tw);
+    for (int i = tid; i < ntw_s; i += blockDim.x) stw_s[i] = twg[i];
+    const C *stw = a.tw_smem ? stw_s : twg;
+    for (int gg = tid; gg < G; gg += blockDim.x) {
+        const long long l = line0 + gg;
+        if (l < a.nlines) {
+            const long long b0 = l % a.c0;
+            const long long r = l / a.c0;
+            const long long b1 = r % a.c1;
+            const long long b2 = r / a.c1;
+            offs[2 * gg] = b0 * a.ib0 + b1 * a.ib1 + b2 * a.ib2;
+            offs[2 * gg + 1] = b0 * a.ob0 + b1 * a.ob1 + b2 * a.ob2;
+            bidx[4 * gg] = (int)b0;
+            bidx[4 * gg + 1] = (int)b1;
+            bidx[4 * gg + 2] = (int)b2;
+            bidx[4 * gg + 3] = 1;
+        } else {
+            offs[2 * gg] = 0;
+            offs[2 * gg + 1] = 0;
+            bidx[4 * gg] = bidx[4 * gg + 1] = bidx[4 * gg + 2] = 0;
+            bidx[4 * gg + 3] = 0;
+        }
+    }
+    __syncthreads();
+
+    const int kind = a.kind;
+    const long long is = a.is, os = a.os;
+
+    // ------------------------------------------------------------ load (asynchronous copies)
+    const void *gdummy = a.in;
+    if (kind == K_C2C_FWD || kind == K_C2C_INV || kind == K_SANDWICH) {
+        const C *in = reinterpret_cast<const C *>(a.in);
+        const int tot = G * NF;
+#pragma unroll 4
+        for (int e = tid; e < tot; e += blockDim.x) {
+            int gg, p;
+            if (a.in_pts_fast) { gg = e / NF; p = e - gg * NF; }
+            else { gg = e & (G - 1); p = e >> gshift; }
+            const bool ok = bidx[4 * gg + 3] != 0;
+            cp_async<sizeof(C)>(&lines[gg * LP + pad16(p)], ok ? (const void *)(in + offs[2 * gg] + p * is) : gdummy,
+                                ok);
+        }
+    } else if (kind == K_R2C) {
+        const R *in = reinterpret_cast<const R *>(a.in);
+        const int tot = G * NF;
+#pragma unroll 4
+        for (int e = tid; e < tot; e += blockDim.x) {
+            int gg, p;
+            if (a.in_pts_fast) { gg = e / NF; p = e - gg * NF; }
+            else { gg = e & (G - 1); p = e >> gshift; }
+            const bool ok = bidx[4 * gg + 3] != 0;
+            C *dst = &lines[gg * LP + pad16(p)];
+            const R *src = in + offs[2 * gg];
+            if (a.half) {
+                if (a.pair_io) {
+                    cp_async<sizeof(C)>(dst, ok ? (const void *)(src + 2 * p) : gdummy, ok);
+                } else {
+                    cp_async<sizeof(R)>(&dst->x, ok ? (const void *)(src + (2 * p) * is) : gdummy, ok);
+                    cp_async<sizeof(R)>(&dst->y, ok ? (const void *)(src + (2 * p + 1) * is) : gdummy, ok);
+                }
+            } else {
+                cp_async<sizeof(R)>(&dst->x, ok ? (const void *)(src + p * is) : gdummy, ok);
+                dst->y = R(0);
+            }
+        }
+    } else { // K_C2R
+        const C *in = reinterpret_cast<const C *>(a.in);
+        const int nin = a.half ? NF + 1 : NF / 2 + 1;
+        const int tot = G * nin;
+#pragma unroll 4
+        for (int e = tid; e < tot; e += blockDim.x) {
+            int gg, p;
+            if (a.in_pts_fast) { gg = e / nin; p = e - gg * nin; }
+            else { gg = e & (G - 1); p = e >> gshift; }
+            const bool ok = bidx[4 * gg + 3] != 0;
+            cp_async<sizeof(C)>(&lines[gg * LP + pad16(p)], ok ? (const void *)(in + offs[2 * gg] + p * is) : gdummy,
+                                ok);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+
+    C *ln = lines + g * LP;
+    const bool active_thread = g < G;
+
+    // ------------------------------------------------------------ C2R pre-processing
+    if (kind == K_C2R) {
+        if (active_thread) {
+            if (a.half) {
+                // Z[k] = E + iO, Z[NF-k] = conj(E - iO) with E = X[k] + conj(X[NF-k]),
+                // O = (X[k] - conj(X[NF-k])) * conj(w_{2NF}^k); DC and Nyquist taken real.
+                for (int k = t; k <= NF / 2; k += T) {
+                    C xk = ln[pad16(k)];
+                    C xm = cconj(ln[pad16(NF - k)]);
+                    if (k == 0) { xk.y = R(0); xm.y = R(0); }
+                    const C e = cadd(xk, xm);
+                    const C o = cmulc(csub(xk, xm), stw[k]);
+                    const C io = mul_si<1>(o);
+                    ln[pad16(k)] = cadd(e, io);
+                    if (k != 0) ln[pad16(NF - k)] = cconj(csub(e, io));
+                }
+            } else {
+                // odd length: Hermitian extension of the half line
+                for (int k = t; k < NF; k += T) {
+                    if (k == 0) { C v = ln[0]; v.y = R(0); ln[0] = v; }
+                    else if (k > NF / 2) ln[pad16(k)] = cconj(ln[pad16(NF - k)]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    // ------------------------------------------------------------ FFT core
+    C *lnp = active_thread ? ln : lines;  // idle threads of a short last CTA still join the barriers
+    if (kind == K_C2C_INV || kind == K_C2R) {
+        fft_line<R, NF, +1>(lnp, stw, a.ntw, active_thread ? t : 0);
+    } else {
+        fft_line<R, NF, -1>(lnp, stw, a.ntw, active_thread ? t : 0);
+    }
+
+    if (kind == K_SANDWICH) {
+        if (active_thread && bidx[4 * g + 3]) {
+            for (int p = t; p < NF; p += T) ln[pad16(p)] = cscale(ln[pad16(p)], ep_factor<R>(a, p, bidx + 4 * g));
+        }
+        __syncthreads();
+        fft_line<R, NF, +1>(lnp, stw, a.ntw, active_thread ? t : 0);
+    }
+
+    // ------------------------------------------------------------ R2C post-processing
+    if (kind == K_R2C && a.half) {
+        if (active_thread) {
+            // X[k] = E + w^k O, X[NF-k] = conj(E - w^k O), E = (Z[k]+conj Z[NF-k])/2, O = -i(Z[k]-conj Z[NF-k])/2
+            for (int k = t; k <= NF / 2; k += T) {
+                const C zk = ln[pad16(k)];
+                const C zm = cconj(ln[pad16(k == 0 ? 0 : NF - k)]);
+                const C e = cscale(cadd(zk, zm), R(0.5));
+                const C o = cscale(mul_si<-1>(csub(zk, zm)), R(0.5));
+                const C w = cmul(o, stw[k]);
+                ln[pad16(k)] = cadd(e, w);
+                ln[pad16(NF - k)] = cconj(csub(e, w));
+            }
+        }
+        __syncthreads();
+    }
+
+    // ------------------------------------------------------------ store
+    const bool ep_store = (a.ep_mode != 0) && kind != K_SANDWICH;
+    if (kind == K_C2R) {
+        R *out = reinterpret_cast<R *>(a.out);
+        const R sc = R(a.ep_scale);
+        if (a.half) {
+            const int tot = G * NF;
+            for (int e = tid; e < tot; e += blockDim.x) {
+                int gg, p;
+                if (a.out_pts_fast) { gg = e / NF; p = e - gg * NF; }
+                else { gg = e & (G - 1); p = e >> gshift; }
+                if (!bidx[4 * gg + 3]) continue;
+                C v = lines[gg * LP + pad16(p)];
+                if (ep_store) v = cscale(v, sc);
+                R *dst = out + offs[2 * gg + 1];
+                if (a.pair_io) *reinterpret_cast<C *>(dst + 2 * p) = v;
+                else { dst[(2 * p) * os] = v.x; dst[(2 * p + 1) * os] = v.y; }
+            }
+        } else {
+            const int tot = G * NF;
+            for (int e = tid; e < tot; e += blockDim.x) {
+                int gg, p;
+                if (a.out_pts_fast) { gg = e / NF; p = e - gg * NF; }
+                else { gg = e & (G - 1); p = e >> gshift; }
+                if (!bidx[4 * gg + 3]) continue;
+                R v = lines[gg * LP + pad16(p)].x;
+                if (ep_store) v *= sc;
+                out[offs[2 * gg + 1] + p * os] = v;
+            }
+        }
+    } else {
+        C *out = reinterpret_cast<C *>(a.out);
+        const int nout = (kind == K_R2C) ? (a.half ? NF + 1 : NF / 2 + 1) : NF;
+        const int tot = G * nout;
+#pragma unroll 4
+        for (int e = tid; e < tot; e += blockDim.x) {
+            int gg, p;
+            if (a.out_pts_fast) { gg = e / nout; p = e - gg * nout; }
+            else { gg = e & (G - 1); p = e >> gshift; }
+            if (!bidx[4 * gg + 3]) continue;
+            C v = lines[gg * LP + pad16(p)];
+            if (ep_store) v = cscale(v, ep_factor<R>(a, p, bidx + 4 * gg));
+            out[offs[2 * gg + 1] + p * os] = v;
+        }
+    }
+}
+
+template <typename R, int NF> inline PassKernelInfo pass_kernel_info()
+{
+    PassKernelInfo k;
+    k.nf = NF;
+    k.threads_per_line = threads_per_line(NF);
+    k.line_pitch = pad16(NF) + 1;
+    k.fn = (const void *)&fftb_pass_kernel<R, NF>;
+    return k;
+}
+
+} // namespace fftb

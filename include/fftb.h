@@ -1,0 +1,162 @@
+/*
+ * fftb.h -- C ABI of the B200-native (sm_100a) replacement for fftm's
+ * single-GPU transform path.
+ *
+ * Two layers are exported, both with plain pointers, sizes and int status codes
+ * (0 = success, negative = error; no exceptions cross the ABI):
+ *
+ *  1. Plan objects that stand in for one `cufft::fft<T, D>` plan of the
+ *     reference's backend (reference source/external_wrap/cufft_wrap.h:456-480,
+ *     483-1282).  Parameters have cuFFT "advanced layout" meaning with 64-bit
+ *     sizes, exactly as fft_wrap_many::add_plan_{1D,2D,3D} passes them
+ *     (source/external_wrap/fft_wrap_many.h:137-186).  Work areas are external
+ *     and optional; streams are per plan.
+ *
+ *  2. `ffts` transform objects that stand in for fftm::ffts<...>
+ *     (source/ffts.hpp:159-383): 2D/3D and 4D R2C forward / C2R inverse with
+ *     the reference's physical array layouts, plus the fused periodic Poisson
+ *     solve of examples/poisson and source/tests/test_{3D,4D}_poisson.cu.
+ *
+ * All execution calls are asynchronous on the object's stream.  Device pointers
+ * only.  One host thread per object (the reference has no internal locking
+ * either, source/ffts.hpp:159).
+ */
+#ifndef FFTB_H
+#define FFTB_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+#define FFTB_SUCCESS 0
+#define FFTB_ERROR_INVALID_VALUE (-1)     /* bad size, stride, direction, dtype, layout */
+#define FFTB_ERROR_UNSUPPORTED_SIZE (-2)  /* a line length the kernels do not cover */
+#define FFTB_ERROR_CUDA (-3)              /* a CUDA runtime call or launch failed */
+#define FFTB_ERROR_ALLOC (-4)             /* device allocation failed */
+#define FFTB_ERROR_INVALID_HANDLE (-5)
+#define FFTB_ERROR_NOT_INITIALIZED (-6)   /* ffts object used before init (source/ffts.hpp:639-645) */
+#define FFTB_ERROR_WRONG_DIMENSION (-7)   /* 3D object used as 4D etc. (source/ffts.hpp:647-657) */
+#define FFTB_ERROR_ALREADY_INITIALIZED (-8) /* init twice (source/ffts.hpp:631-637) */
+#define FFTB_ERROR_MISALIGNED (-9)        /* pointer not aligned to its element type */
+#define FFTB_ERROR_NO_WORK_AREA (-10)     /* work area required but missing */
+
+/* direction values equal fftm::direction (source/fft_direction.h:9-15) */
+#define FFTB_R2C 1
+#define FFTB_C2R 2
+#define FFTB_C2CF 3
+#define FFTB_C2CB 4
+
+#define FFTB_F32 0
+#define FFTB_F64 1
+
+/* 4D layouts:
+ *  PENCIL      ffts<..., strategy_4d_pencil_pencil>: real [w][z][y][x] -> spectrum [ky][kz][kw<nw/2+1][kx]
+ *              (source/ffts.hpp:126-134, 809-825)
+ *  SLAB        ffts<..., strategy_4d_slab_slab>:     real [x][y][z][w] -> spectrum [kx][ky][kz][kw<nw/2+1]
+ *              (source/ffts.hpp:144-150, 827-837)
+ *  NATIVE_XZWY fftm slab with fftm_4d_spectral_layout::native_xzwy: real [x][y][z][w] -> spectrum
+ *              [ky][kz][kw<nw/2+1][kx] (source/fftm_options.hpp:48-52, source/fftm.hpp:2941-2961) */
+#define FFTB_4D_PENCIL 0
+#define FFTB_4D_SLAB 1
+#define FFTB_4D_NATIVE_XZWY 2
+
+const char *fftb_status_string(int status);
+/* detail message of the last failing call on this host thread ("" if none) */
+const char *fftb_last_error_message(void);
+/* library version "major.minor.patch" */
+const char *fftb_version(void);
+
+/* ------------------------------------------------------------------ plans */
+typedef struct fftb_plan_s *fftb_plan;
+
+/* Replaces cufft::fft<T,D>::fft(n, inembed, istride, idist, onembed, ostride, odist,
+ * batch) -> create_plan -> cufftMakePlanMany64 (source/external_wrap/cufft_wrap.h:533-566,
+ * :1237-1259).  inembed/onembed may be NULL for the default tight layout
+ * (cufft_wrap.h:568-587).  *work_bytes receives the work-area size (may be 0). */
+int fftb_plan_create(int direction, int dtype, int rank, const long long *n, const long long *inembed,
+                     long long istride, long long idist, const long long *onembed, long long ostride,
+                     long long odist, long long batch, fftb_plan *plan, size_t *work_bytes);
+/* Replaces fft_base::get_work_size (cufft_wrap.h:599-602) */
+int fftb_plan_get_work_size(fftb_plan plan, size_t *work_bytes);
+/* Replaces fft_base::set_work_area (cufft_wrap.h:605-609) */
+int fftb_plan_set_work_area(fftb_plan plan, void *work_area);
+/* Replaces fft_base::set_stream (cufft_wrap.h:611-615); stream is a cudaStream_t */
+int fftb_plan_set_stream(fftb_plan plan, void *stream);
+/* Replaces fft_base::exec / exec_no_sync (cufft_wrap.h:649-662): asynchronous.
+ * Multi-dimensional C2R plans overwrite `in`, as cuFFT's do. */
+int fftb_exec(fftb_plan plan, void *in, void *out);
+/* Replaces fft_base::exec_direction (cufft_wrap.h:664-700): a C2C plan may run
+ * either sign; R2C/C2R plans only their own direction. */
+int fftb_exec_direction(fftb_plan plan, int direction, void *in, void *out);
+/* Replaces fft_base::get_direction / descriptor (cufft_wrap.h:470-472,
+ * source/external_wrap/fft_plan_descriptor.h:15-32).  Arrays have 3 entries. */
+int fftb_plan_describe(fftb_plan plan, int *direction, int *dtype, int *rank, long long *n, long long *inembed,
+                       long long *istride, long long *idist, long long *onembed, long long *ostride,
+                       long long *odist, long long *batch);
+/* number of kernel launches one exec issues */
+int fftb_plan_num_launches(fftb_plan plan, int *launches);
+/* Replaces ~fft (cufft_wrap.h:589-595) */
+int fftb_plan_destroy(fftb_plan plan);
+
+/* ------------------------------------------------------------------ ffts transforms */
+typedef struct fftb_ffts_s *fftb_ffts;
+
+/* ffts() + ffts::init(nx, ny[, nz[, nw]]) (source/ffts.hpp:192-285).  layout4d is
+ * one of FFTB_4D_* and ignored for 2D/3D.  nz = nw = 0 selects 2D; nw = 0 3D. */
+int fftb_ffts_create(int dtype, long long nx, long long ny, long long nz, long long nw, int layout4d,
+                     fftb_ffts *obj);
+int fftb_ffts_destroy(fftb_ffts obj);
+/* ffts::dimension (source/ffts.hpp:330-334) */
+int fftb_ffts_dimension(fftb_ffts obj, int *dim);
+/* Work bytes the object needs for forward/backward/poisson (the reference's shared
+ * work buffer plus 4D stage scratch, source/ffts.hpp:439-447, 778-796). */
+int fftb_ffts_work_size(fftb_ffts obj, size_t *work_bytes);
+/* Supplies the work area (caller-owned, >= work_size bytes, 256-byte aligned).  If
+ * never called, the first execution that needs scratch allocates it. */
+int fftb_ffts_set_work_area(fftb_ffts obj, void *work);
+int fftb_ffts_set_stream(fftb_ffts obj, void *stream);
+/* ffts::forward (source/ffts.hpp:338-375): unnormalised R2C, e^{-i theta}. */
+int fftb_ffts_forward(fftb_ffts obj, const void *real_in, void *complex_out);
+/* ffts::backward (source/ffts.hpp:344-383): unnormalised C2R, e^{+i theta}.
+ * `complex_in` may be overwritten (the reference's 3D/4D backward is destructive). */
+int fftb_ffts_backward(fftb_ffts obj, void *complex_in, void *real_out);
+/* backward followed by the 1/N scale of the reference drivers
+ * (source/tests/detail/fft_benchmark_common.h:271-281), fused into the last pass. */
+int fftb_ffts_backward_normalized(fftb_ffts obj, void *complex_in, void *real_out);
+/* Periodic spectral Poisson solve on [0, 2pi)^d with integer wavenumbers:
+ * u = C2R( sign * R2C(f) / |k|^2 ) / N, k = 0 mode set to 0.  sign = -1 solves
+ * lap u = f (source/tests/test_3D_poisson.cu:82-111), sign = +1 solves -lap u = f
+ * (examples/poisson/source/poisson_periodic_3d_autotuned.cpp:74-103).  The
+ * multiply is fused into the FFT passes; the spectrum lives in the work area.
+ * rhs and solution may alias. */
+int fftb_ffts_poisson(fftb_ffts obj, const void *rhs, void *solution, double sign);
+/* Spectral filter round trip: u = C2R( G(k) * R2C(f) ) / N with the Gaussian
+ * G(k) = exp(-|k|^2 / (2 sigma^2)); optionally followed in the same fused pass by
+ * the Poisson multiply (poisson_sign = 0 disables it). */
+int fftb_ffts_filter(fftb_ffts obj, const void *in, void *out, double sigma, double poisson_sign);
+/* In-place spectral multiplies on a spectrum in this object's layout (the
+ * reference's standalone functors): Poisson sign/|k|^2 (k=0 -> 0) with an extra
+ * scale, examples/poisson/source/poisson_periodic_{3d,4d}_autotuned.cpp. */
+int fftb_ffts_spectrum_poisson(fftb_ffts obj, void *spectrum, double sign, double scale);
+/* number of kernel launches of forward (which=0) / backward (1) / poisson (2) / filter (3) */
+int fftb_ffts_num_launches(fftb_ffts obj, int which, int *launches);
+/* Profiling hook (the role of the reference's ffts profiler, source/ffts.hpp:64-72,
+ * 449-629, but timed on the device): with max_launches > 0, every later execution
+ * records a CUDA event on the object's stream before each kernel launch and after
+ * the last, for up to max_launches launches; 0 disables and frees the events. */
+int fftb_ffts_timing_enable(fftb_ffts obj, int max_launches);
+/* Waits for the recorded events and returns, per recorded launch in issue order, its
+ * device time in ms, its algorithmic bytes (one read of its input and one write of
+ * its output) and its kernel name (NUL-terminated, name_stride bytes per entry).
+ * Clears the record. */
+int fftb_ffts_timing_read(fftb_ffts obj, float *ms, double *bytes, char *names, int name_stride, int cap,
+                          int *count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FFTB_H */
