@@ -134,6 +134,15 @@ bool has_kernel(int dtype, int nf)
     return r.tab[dtype].count(nf) != 0;
 }
 
+bool lookup_kernel(int dtype, int nf, PassKernelInfo *out)
+{
+    Registry &r = reg();
+    auto it = r.tab[dtype].find(nf);
+    if (it == r.tab[dtype].end()) return false;
+    *out = it->second;
+    return true;
+}
+
 int program_add(Program &prog, int dtype, const AxisPass &p)
 {
     if (p.n < 1) return FFTB_ERROR_INVALID_VALUE;

@@ -101,6 +101,8 @@ int timer_end(LaunchTimer *t, cudaStream_t s);
 
 // true if a line of complex length nf has a compiled kernel for dtype
 bool has_kernel(int dtype, int nf);
+// copies the registry entry of the pass kernel for (dtype, nf); false if none
+bool lookup_kernel(int dtype, int nf, PassKernelInfo *out);
 
 // element size of the complex type
 inline size_t complex_bytes(int dtype) { return dtype == 0 ? 8 : 16; }

@@ -155,6 +155,35 @@ int fftb_ffts_timing_enable(fftb_ffts obj, int max_launches);
 int fftb_ffts_timing_read(fftb_ffts obj, float *ms, double *bytes, char *names, int name_stride, int cap,
                           int *count);
 
+/* ------------------------------------------------------------------ allocation-free entry point */
+/* Bytes of the spectrum scratch that fftb_poisson3d_f32_noalloc keeps in static
+ * device memory (nx * ny * (nz/2+1) * 8 must not exceed it). */
+#define FFTB_NOALLOC_MAX_SPECTRUM_BYTES (16u * 1024u * 1024u)
+
+/* 3D periodic Poisson solve in float32 that allocates no device memory, for
+ * callers that cannot call cudaMalloc: a framework or serving process whose
+ * memory pool owns the device, or a job that must not allocate (and so must not
+ * risk the implicit synchronisation of cudaMalloc/cudaFree) between steps.  No
+ * counterpart in the reference, whose ffts allocates its work buffer
+ * (source/ffts.hpp:439-447).
+ *
+ * Same result as fftb_ffts_poisson on a float32 [x][y][z] field: u = C2R(sign *
+ * R2C(f) / |k|^2) / N with k = 0 set to 0.  rhs and solution are caller-owned
+ * device arrays of nx*ny*nz floats (they may alias); stream is a cudaStream_t
+ * (NULL: the legacy default stream).  2 <= nx, ny, nz <= 4096, every length a
+ * supported line length, and the spectrum at most FFTB_NOALLOC_MAX_SPECTRUM_BYTES
+ * (e.g. 128^3); larger sizes return FFTB_ERROR_INVALID_VALUE.
+ *
+ * The scratch (twiddle tables and spectrum) is one static __device__ array that
+ * every GPU loading the library holds until the process exits.  The first call on
+ * a device looks up its address (cudaGetSymbolAddress) for that device; make that
+ * first call before any stream capture.  All calls share the array and it keeps
+ * the last call's contents (each call rewrites what it reads), so calls whose
+ * executions overlap on the GPU -- on different streams, or from different host
+ * threads -- race on it and must be serialised by the caller. */
+int fftb_poisson3d_f32_noalloc(const float *rhs, float *solution, long long nx, long long ny, long long nz,
+                               double sign, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
