@@ -134,6 +134,8 @@ bool has_kernel(int dtype, int nf)
     return r.tab[dtype].count(nf) != 0;
 }
 
+int engine_roots(int dtype, int ntw, void **out) { return get_roots(dtype, ntw, out); }
+
 bool lookup_kernel(int dtype, int nf, PassKernelInfo *out)
 {
     Registry &r = reg();

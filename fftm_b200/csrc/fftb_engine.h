@@ -99,6 +99,9 @@ int program_exec(const Program &prog, void *in, void *out, void *work, cudaStrea
 int timer_mark(LaunchTimer *t, cudaStream_t s, const std::string &name, double bytes);
 int timer_end(LaunchTimer *t, cudaStream_t s);
 
+// device table of the forward roots exp(-2 pi i m / ntw), shared per (device, dtype, ntw)
+int engine_roots(int dtype, int ntw, void **out);
+
 // true if a line of complex length nf has a compiled kernel for dtype
 bool has_kernel(int dtype, int nf);
 // copies the registry entry of the pass kernel for (dtype, nf); false if none

@@ -1,8 +1,549 @@
-// fftb_fused3d.cu -- specialised fused 3D kernels.
+// fftb_fused3d.cu -- specialised 3D kernels for power-of-two sizes.
+//
+// A 3D R2C + C2R round trip (and the Poisson solve between them) runs as three
+// kernels instead of the reference's cuFFT 3D plan plus separate multiply and
+// scale kernels:
+//
+//   plane_fwd  per x-plane: R2C of every z row, then the FFT of every kz column
+//              over y; writes the plane [ky][kz] of the spectrum.
+//   xcol       per tile of W spectrum columns (ky,kz): the x FFT (forward,
+//              inverse, or forward -> spectral multiply -> inverse).
+//   plane_inv  per x-plane: inverse FFT over y, then C2R of every row, times a
+//              scale (1/N for the normalised inverse and the Poisson solve).
+//
+// All FFTs are register resident (fftb_regfft.cuh); shared memory holds the
+// plane between the z and y stages.  A 256x256 plane (133 KB of spectrum) is
+// split over a 2-CTA cluster: each CTA transforms half of the rows along z, and
+// the y FFT's first radix-2 step is taken across the pair through distributed
+// shared memory (CTA 0 forms x[m] + x[m+M] and yields the even ky, CTA 1 forms
+// (x[m] - x[m+M]) w^m and yields the odd ky), so no plane ever round-trips
+// through global memory between the z and y stages.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <cstdlib>
+#include <string>
+
 #include "../../include/fftb.h"
 #include "fftb_fused3d.h"
+#include "fftb_regfft.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace fftb {
+
+// ------------------------------------------------------------------ plane kernels
+// Work split (CL CTAs per plane, CL in {1, 2}):
+//   rows   : CTA c owns rows [c*M, (c+1)*M) for the z stage            (M = NY / CL)
+//   columns: CTA c owns column slots [c*S, (c+1)*S) for the y stage     (S = NZ / (2 CL))
+// Slot s < NZ/2 is spectrum column kz = s, except slot 0, which packs the two
+// real-per-row columns kz = 0 and kz = NZ/2 as one complex column (kz=0 in the
+// real part, kz=NZ/2 in the imaginary part); their y FFTs are separated by
+// Hermitian symmetry (forward) or simply stay packed (inverse, where the C2R
+// keeps only the real parts of kz = 0 and NZ/2).  Data that changes owner
+// between the stages is pushed with distributed-shared-memory stores, so no CTA
+// ever reads another CTA's shared memory.
+template <int NY, int NZ, int CL> struct PlaneShape {
+    static constexpr int NT = CL > 1 ? 512 : 256;            // threads per CTA
+    static constexpr int M = NY / CL;                        // rows per CTA (z stage)
+    static constexpr int S = NZ / (2 * CL);                  // column slots per CTA (y stage)
+    static constexpr int NS = NZ / 2;                        // slots of the plane
+    static constexpr int TZ = RegFFTShape<NZ>::T;
+    static constexpr int TY = RegFFTShape<NY>::T;
+    static constexpr int FZ = NT / TZ, FY = NT / TY;         // concurrent FFTs per stage
+    static constexpr int NMAX = NY > NZ ? NY : NZ;
+    // forward: y-stage plane [NY][PF], PF = 16/TY (mod 16) -> conflict-free column reads
+    static constexpr int PMOD = 16 / TY;
+    static constexpr int PF = S + ((PMOD - S % 16) % 16 + 16) % 16;
+    static constexpr int SCR_Z = FZ * RegFFTShape<NZ>::REGION;
+    static constexpr int SCR_Y = FY * RegFFTShape<NY>::REGION;
+    static constexpr int SCRF = SCR_Z > SCR_Y ? SCR_Z : SCR_Y;
+    // inverse: z-stage rows [M][PR] (PR odd -> conflict-free column pushes) and a
+    // column-major staging area of FY columns of PC entries (PC odd, >= REGION)
+    static constexpr int PR = NS + 1;
+    static constexpr int REGY = RegFFTShape<NY>::REGION > NY ? RegFFTShape<NY>::REGION : NY;
+    static constexpr int PC = REGY | 1;
+    static constexpr int STG = FY * PC > SCR_Z ? FY * PC : SCR_Z;
+    template <typename R> static constexpr size_t smem_fwd()
+    {
+        return sizeof(cpx<R>) * ((size_t)NY * PF + SCRF + NMAX);
+    }
+    template <typename R> static constexpr size_t smem_inv()
+    {
+        return sizeof(cpx<R>) * ((size_t)M * PR + STG + NMAX);
+    }
+};
+
+template <typename R, int NY, int NZ, int CL>
+__global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT)
+    plane_fwd_kernel(const R *__restrict__ in, cpx<R> *__restrict__ out, const cpx<R> *__restrict__ roots)
+{
+    using C = cpx<R>;
+    using S = PlaneShape<NY, NZ, CL>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *plane = reinterpret_cast<C *>(smem_raw);   // [NY][PF]: this CTA's column slots
+    C *scr = plane + NY * S::PF;
+    C *tw = scr + S::SCRF;
+    const int tid = threadIdx.x;
+    const int c = (CL > 1) ? (int)cg::this_cluster().block_rank() : 0;
+    const int x = (int)(blockIdx.x / CL);
+    C *dst[2] = {plane, plane};
+    if constexpr (CL > 1) {
+        dst[0] = cg::this_cluster().map_shared_rank(plane, 0u);
+        dst[1] = cg::this_cluster().map_shared_rank(plane, 1u);
+    }
+    for (int i = tid; i < S::NMAX; i += S::NT) tw[i] = roots[i];
+    __syncthreads();
+
+    // ---- stage z: R2C of this CTA's rows (two rows per complex FFT), pushed to the slot owners
+    {
+        constexpr int TZ = S::TZ, FZ = S::FZ;
+        const int f = tid / TZ, t = tid - (tid / TZ) * TZ;
+        C *reg = scr + f * RegFFTShape<NZ>::REGION;
+        const R *rows = in + ((size_t)x * NY + (size_t)c * S::M) * NZ;
+#pragma unroll 1
+        for (int p0 = 0; p0 < S::M / 2; p0 += FZ) {
+            const int p = p0 + f;
+            const bool ok = p < S::M / 2;
+            const int pp = ok ? p : 0;
+            const R *ra = rows + (size_t)(2 * pp) * NZ;
+            const R *rb = ra + NZ;
+            C v[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                v[r].x = ra[t + TZ * r];
+                v[r].y = rb[t + TZ * r];
+            }
+            regfft_warp<R, NZ, -1>(v, reg, tw, S::NMAX / NZ, t);
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < 16; ++j) reg[t + TZ * j] = v[j];
+            __syncwarp();
+            if (ok) {
+                const int ya = c * S::M + 2 * pp;  // row index within the plane
+#pragma unroll
+                for (int j = 0; j < NZ / (2 * TZ); ++j) {
+                    const int k = t + TZ * j;      // k < NZ/2
+                    const C zk = reg[k];
+                    const C zm = cconj(reg[(NZ - k) & (NZ - 1)]);
+                    C A = cscale(cadd(zk, zm), R(0.5));
+                    C B = cscale(mul_si<-1>(csub(zk, zm)), R(0.5));
+                    if (k == 0) {
+                        // pack kz = 0 (real) and kz = NZ/2 (real) into slot 0
+                        const C zn = reg[NZ / 2];
+                        A = mk<R>(zk.x, zn.x);
+                        B = mk<R>(zk.y, zn.y);
+                    }
+                    const int owner = k / S::S, ls = k - owner * S::S;
+                    C *d = dst[CL > 1 ? owner : 0];
+                    d[ya * S::PF + ls] = A;
+                    d[(ya + 1) * S::PF + ls] = B;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if constexpr (CL > 1) cg::this_cluster().sync();
+    else __syncthreads();
+
+    // ---- stage y: FFT over the NY rows of every owned slot, in place
+    {
+        constexpr int TY = S::TY, FY = S::FY;
+        const int f = tid / TY, t = tid - (tid / TY) * TY;
+        C *reg = scr + f * RegFFTShape<NY>::REGION;
+        C *oplane = out + (size_t)x * NY * (NZ / 2 + 1);
+#pragma unroll 1
+        for (int s0 = 0; s0 < S::S; s0 += FY) {
+            const int sl = s0 + f;
+            const bool ok = sl < S::S;
+            const int slc = ok ? sl : 0;
+            C v[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) v[r] = plane[(t + TY * r) * S::PF + slc];
+            regfft_warp<R, NY, -1>(v, reg, tw, S::NMAX / NY, t);
+            // the packed slot: X0[ky] = (W[ky] + conj W[-ky]) / 2, XN[ky] = (W[ky] - conj W[-ky]) / 2i
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < 16; ++j) reg[t + TY * j] = v[j];
+            __syncwarp();
+            if (ok && c == 0 && sl == 0) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int ky = t + TY * j;
+                    const C wk = v[j];
+                    const C wm = cconj(reg[(NY - ky) & (NY - 1)]);
+                    v[j] = cscale(cadd(wk, wm), R(0.5));
+                    oplane[(size_t)ky * (NZ / 2 + 1) + NZ / 2] = cscale(mul_si<-1>(csub(wk, wm)), R(0.5));
+                }
+            }
+            if (ok) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) plane[(t + TY * j) * S::PF + slc] = v[j];
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    // ---- coalesced row stores of the owned slots: out[x][ky][c*S + s]
+    {
+        C *oplane = out + (size_t)x * NY * (NZ / 2 + 1) + c * S::S;
+#pragma unroll 4
+        for (int e = tid; e < NY * S::S; e += S::NT) {
+            const int row = e / S::S, sl = e - (e / S::S) * S::S;
+            oplane[(size_t)row * (NZ / 2 + 1) + sl] = plane[row * S::PF + sl];
+        }
+    }
+}
+
+template <typename R, int NY, int NZ, int CL>
+__global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT)
+    plane_inv_kernel(const cpx<R> *__restrict__ in, R *__restrict__ out, const cpx<R> *__restrict__ roots, R scale)
+{
+    using C = cpx<R>;
+    using S = PlaneShape<NY, NZ, CL>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *rowsm = reinterpret_cast<C *>(smem_raw);   // [M][PR]: this CTA's rows, every slot
+    C *stg = rowsm + S::M * S::PR;                // staging columns / FFT exchange regions
+    C *tw = stg + S::STG;
+    const int tid = threadIdx.x;
+    const int c = (CL > 1) ? (int)cg::this_cluster().block_rank() : 0;
+    const int x = (int)(blockIdx.x / CL);
+    C *dst[2] = {rowsm, rowsm};
+    if constexpr (CL > 1) {
+        dst[0] = cg::this_cluster().map_shared_rank(rowsm, 0u);
+        dst[1] = cg::this_cluster().map_shared_rank(rowsm, 1u);
+    }
+    for (int i = tid; i < S::NMAX; i += S::NT) tw[i] = roots[i];
+    const C *iplane = in + (size_t)x * NY * (NZ / 2 + 1);
+
+    // ---- stage y: inverse FFT of the owned slots, rows pushed to their owners
+    {
+        constexpr int TY = S::TY, FY = S::FY;
+        const int f = tid / TY, t = tid - (tid / TY) * TY;
+#pragma unroll 1
+        for (int s0 = 0; s0 < S::S; s0 += FY) {
+            const int ns = (S::S - s0) < FY ? (S::S - s0) : FY;
+            // stage ns columns (all NY rows) with coalesced asynchronous copies
+            for (int e = tid; e < NY * ns; e += S::NT) {
+                const int row = e / ns, sl = e - (e / ns) * ns;
+                cp_async<sizeof(C)>(&stg[sl * S::PC + row],
+                                    iplane + (size_t)row * (NZ / 2 + 1) + c * S::S + s0 + sl, true);
+            }
+            cp_async_wait_all();
+            __syncthreads();
+            const int sl = s0 + f;
+            const bool ok = f < ns;
+            C *col = stg + f * S::PC;  // every group owns a column slot (idle ones compute on stale data)
+            C v[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) v[r] = col[t + TY * r];
+            if (ok && c == 0 && sl == 0) {
+                // packed slot: W = X0 + i XN
+#pragma unroll
+                for (int r = 0; r < 16; ++r) {
+                    const C xn = iplane[(size_t)(t + TY * r) * (NZ / 2 + 1) + NZ / 2];
+                    v[r] = mk<R>(v[r].x - xn.y, v[r].y + xn.x);
+                }
+            }
+            __syncwarp();
+            regfft_warp<R, NY, +1>(v, col, tw, S::NMAX / NY, t);
+            if (ok) {
+                const int gs = c * S::S + sl;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int m = t + TY * j;
+                    const int owner = m / S::M;
+                    C *d = dst[CL > 1 ? owner : 0];
+                    d[(m - owner * S::M) * S::PR + gs] = v[j];
+                }
+            }
+            __syncthreads();  // the staging area is reused by the next round
+        }
+    }
+    if constexpr (CL > 1) cg::this_cluster().sync();
+    else __syncthreads();
+
+    // ---- stage z: C2R of two rows per complex FFT
+    {
+        constexpr int TZ = S::TZ, FZ = S::FZ;
+        const int f = tid / TZ, t = tid - (tid / TZ) * TZ;
+        C *reg = stg + f * RegFFTShape<NZ>::REGION;
+        R *rows = out + ((size_t)x * NY + (size_t)c * S::M) * NZ;
+#pragma unroll 1
+        for (int p0 = 0; p0 < S::M / 2; p0 += FZ) {
+            const int p = p0 + f;
+            const bool ok = p < S::M / 2;
+            const int pp = ok ? p : 0;
+            const C *ha_row = rowsm + (2 * pp) * S::PR;
+            const C *hb_row = ha_row + S::PR;
+            C v[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                const int n = t + TZ * r;
+                const bool hi = n > NZ / 2;
+                const int k = hi ? NZ - n : n;
+                C ha, hb;
+                if (k == 0 || k == NZ / 2) {
+                    // slot 0 holds kz = 0 in .x and kz = NZ/2 in .y (both real)
+                    const C pa = ha_row[0], pb = hb_row[0];
+                    ha = mk<R>(k == 0 ? pa.x : pa.y, R(0));
+                    hb = mk<R>(k == 0 ? pb.x : pb.y, R(0));
+                } else {
+                    ha = ha_row[k];
+                    hb = hb_row[k];
+                    if (hi) { ha = cconj(ha); hb = cconj(hb); }
+                }
+                v[r] = mk<R>(ha.x - hb.y, ha.y + hb.x);  // Ha + i Hb
+            }
+            regfft_warp<R, NZ, +1>(v, reg, tw, S::NMAX / NZ, t);
+            if (ok) {
+                R *ra = rows + (size_t)(2 * pp) * NZ;
+                R *rb = ra + NZ;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    ra[t + TZ * j] = v[j].x * scale;
+                    rb[t + TZ * j] = v[j].y * scale;
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// ------------------------------------------------------------------ x column kernel
+// Columns c in [0, ncols) of a spectrum whose x rows are `stride` apart.  Thread
+// (t, col) = (tid / W, tid % W) holds rows t + T*r of column col, so every load
+// and store instruction of a warp touches W (or 32) consecutive columns.
+struct XColEp {
+    int mode;  // EpMode bits (0: none)
+    float scale_f, sign_f, gauss_f;
+    double scale, sign, gauss;
+    int nzh, ny, nz;
+};
+
+template <int NX> struct XColShape {
+    static constexpr int T = RegFFTShape<NX>::T;
+    static constexpr int W = 256 / T;      // columns per CTA
+    static constexpr int NT = 256;
+};
+
+template <typename R, int NX, int SIGN>
+__device__ __forceinline__ void xcol_fft(cpx<R> (&v)[16], cpx<R> *scr, const cpx<R> *tw, int t, int col)
+{
+    using C = cpx<R>;
+    constexpr int T = XColShape<NX>::T, W = XColShape<NX>::W;
+    dft16<SIGN, C, R>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < 16; ++k1) v[k1] = twiddle_mul<SIGN>(v[k1], tw, t * k1);
+    __syncthreads();
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) scr[(k1 * T + t) * W + col] = v[k1];
+    __syncthreads();
+    constexpr int A = 16 / T;
+#pragma unroll
+    for (int a = 0; a < A; ++a) {
+        C u[T];
+#pragma unroll
+        for (int q = 0; q < T; ++q) u[q] = scr[((t + T * a) * T + q) * W + col];
+        dft_small<SIGN, T, C, R>(u);
+#pragma unroll
+        for (int k2 = 0; k2 < T; ++k2) v[a + A * k2] = u[k2];
+    }
+}
+
+template <typename R, int NX, int MODE>  // MODE 0: forward, 1: inverse, 2: forward-multiply-inverse
+__global__ void __launch_bounds__(256) xcol_kernel(cpx<R> *__restrict__ data, long long stride, int ncols,
+                                                   const cpx<R> *__restrict__ roots, XColEp ep)
+{
+    using C = cpx<R>;
+    constexpr int T = XColShape<NX>::T, W = XColShape<NX>::W;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *scr = reinterpret_cast<C *>(smem_raw);
+    C *tw = scr + 16 * T * W;
+    const int tid = threadIdx.x;
+    const int t = tid / W, col = tid - (tid / W) * W;
+    for (int i = tid; i < NX; i += 256) tw[i] = roots[i];
+    const int cg0 = blockIdx.x * W + col;
+    const bool ok = cg0 < ncols;
+    C *p = data + (ok ? cg0 : 0);
+    C v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = p[(size_t)(t + T * r) * stride];
+    __syncthreads();
+    if (MODE == 1) xcol_fft<R, NX, +1>(v, scr, tw, t, col);
+    else xcol_fft<R, NX, -1>(v, scr, tw, t, col);
+    if (MODE == 2) {
+        // wavenumbers: kx = t + T*j (output row), ky = col / nzh, kz = col % nzh (half axis)
+        const int ky_i = cg0 / ep.nzh, kz = cg0 - (cg0 / ep.nzh) * ep.nzh;
+        const int ky = ky_i <= ep.ny / 2 ? ky_i : ky_i - ep.ny;
+        const R kyz = R(ky * ky + kz * kz);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int kxi = t + T * j;
+            const int kx = kxi <= NX / 2 ? kxi : kxi - NX;
+            const R k2 = R(kx * kx) + kyz;
+            R fct = sizeof(R) == 4 ? R(ep.scale_f) : R(ep.scale);
+            if (ep.mode & EP_POISSON) {
+                const R sg = sizeof(R) == 4 ? R(ep.sign_f) : R(ep.sign);
+                fct = (k2 == R(0)) ? R(0) : fct * sg / k2;
+            }
+            if (ep.mode & EP_GAUSS) fct *= exp(-k2 * (sizeof(R) == 4 ? R(ep.gauss_f) : R(ep.gauss)));
+            v[j] = cscale(v[j], fct);
+        }
+        xcol_fft<R, NX, +1>(v, scr, tw, t, col);
+    }
+    if (ok) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) p[(size_t)(t + T * j) * stride] = v[j];
+    }
+}
+
+// ------------------------------------------------------------------ host side
+namespace {
+
+struct PlaneEntry {
+    int dtype, ny, nz, cl, nt;
+    const void *fwd, *inv;
+    size_t smem_fwd, smem_inv;
+};
+
+template <typename R, int NY, int NZ, int CL> PlaneEntry plane_entry(int dtype)
+{
+    using S = PlaneShape<NY, NZ, CL>;
+    return PlaneEntry{dtype, NY, NZ, CL, S::NT, (const void *)&plane_fwd_kernel<R, NY, NZ, CL>,
+                      (const void *)&plane_inv_kernel<R, NY, NZ, CL>, S::template smem_fwd<R>(),
+                      S::template smem_inv<R>()};
+}
+
+#define FFTB_PLANES(R, D)                                                                                          \
+    plane_entry<R, 64, 64, 1>(D), plane_entry<R, 64, 64, 2>(D), plane_entry<R, 64, 128, 1>(D),                    \
+        plane_entry<R, 64, 128, 2>(D), plane_entry<R, 64, 256, 1>(D), plane_entry<R, 64, 256, 2>(D),              \
+        plane_entry<R, 128, 64, 1>(D), plane_entry<R, 128, 64, 2>(D), plane_entry<R, 128, 128, 1>(D),             \
+        plane_entry<R, 128, 128, 2>(D), plane_entry<R, 128, 256, 1>(D), plane_entry<R, 128, 256, 2>(D),           \
+        plane_entry<R, 256, 64, 1>(D), plane_entry<R, 256, 64, 2>(D), plane_entry<R, 256, 128, 1>(D),             \
+        plane_entry<R, 256, 128, 2>(D), plane_entry<R, 256, 256, 2>(D)
+
+const PlaneEntry *find_plane(int dtype, int ny, int nz, int cl)
+{
+    static const PlaneEntry tab[] = {FFTB_PLANES(float, FFTB_F32)};
+    for (const PlaneEntry &e : tab)
+        if (e.dtype == dtype && e.ny == ny && e.nz == nz && e.cl == cl) return &e;
+    return nullptr;
+}
+
+struct XColEntry {
+    int dtype, nx;
+    const void *fn[3];
+    size_t smem;
+};
+
+template <typename R, int NX> XColEntry xcol_entry(int dtype)
+{
+    constexpr int T = XColShape<NX>::T, W = XColShape<NX>::W;
+    return XColEntry{dtype,
+                     NX,
+                     {(const void *)&xcol_kernel<R, NX, 0>, (const void *)&xcol_kernel<R, NX, 1>,
+                      (const void *)&xcol_kernel<R, NX, 2>},
+                     sizeof(cpx<R>) * ((size_t)16 * T * W + NX)};
+}
+
+const XColEntry *find_xcol(int dtype, int nx)
+{
+    static const XColEntry tab[] = {xcol_entry<float, 32>(FFTB_F32), xcol_entry<float, 64>(FFTB_F32),
+                                    xcol_entry<float, 128>(FFTB_F32), xcol_entry<float, 256>(FFTB_F32)};
+    for (const XColEntry &e : tab)
+        if (e.dtype == dtype && e.nx == nx) return &e;
+    return nullptr;
+}
+
+int configure(const void *fn, size_t smem)
+{
+    if (smem > 48 * 1024)
+        return set_status_from_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return FFTB_SUCCESS;
+}
+
+int launch_plane(const Fused3D &f, bool inverse, const void *in, void *out, double scale, cudaStream_t s,
+                 LaunchTimer *tm)
+{
+    const PlaneEntry *e = (const PlaneEntry *)f.plane;
+    void *roots = f.roots_plane;
+    float sc = (float)scale;
+    const void *fn = inverse ? e->inv : e->fwd;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(f.nx * e->cl));
+    cfg.blockDim = dim3(e->nt);
+    cfg.dynamicSmemBytes = inverse ? e->smem_inv : e->smem_fwd;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    cfg.attrs = attr;
+    cfg.numAttrs = 0;
+    if (e->cl > 1) {
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = e->cl;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.numAttrs = 1;
+    }
+    const double bytes = (double)f.nx * f.ny * (4.0 * f.nz + 8.0 * (f.nz / 2 + 1));
+    if (tm) {
+        int st = timer_mark(tm, s,
+                            std::string(inverse ? "plane_inv_kernel" : "plane_fwd_kernel") + "<f32," +
+                                std::to_string(f.ny) + "," + std::to_string(f.nz) + ",cl" + std::to_string(e->cl) +
+                                ">",
+                            bytes);
+        if (st != FFTB_SUCCESS) return st;
+    }
+    cudaError_t err;
+    if (inverse) {
+        const float2 *a0 = (const float2 *)in;
+        float *a1 = (float *)out;
+        const float2 *a2 = (const float2 *)roots;
+        void *args[] = {&a0, &a1, &a2, &sc};
+        err = cudaLaunchKernelExC(&cfg, fn, args);
+    } else {
+        const float *a0 = (const float *)in;
+        float2 *a1 = (float2 *)out;
+        const float2 *a2 = (const float2 *)roots;
+        void *args[] = {&a0, &a1, &a2};
+        err = cudaLaunchKernelExC(&cfg, fn, args);
+    }
+    return set_status_from_cuda(err);
+}
+
+int launch_xcol(const Fused3D &f, int mode, void *data, const EpValues *ep, cudaStream_t s, LaunchTimer *tm)
+{
+    const XColEntry *e = (const XColEntry *)f.xcol;
+    const long long nzh = f.nz / 2 + 1;
+    const long long ncols = f.ny * nzh;
+    const int W = 256 / (int)(f.nx / 16);
+    XColEp x = {};
+    x.mode = ep ? (ep->mode < 0 ? 0 : ep->mode) : 0;
+    x.scale = ep ? ep->scale : 1.0;
+    x.sign = ep ? ep->sign : -1.0;
+    x.gauss = ep ? ep->gauss : 0.0;
+    x.scale_f = (float)x.scale;
+    x.sign_f = (float)x.sign;
+    x.gauss_f = (float)x.gauss;
+    x.nzh = (int)nzh;
+    x.ny = (int)f.ny;
+    x.nz = (int)f.nz;
+    if (tm) {
+        static const char *mn[] = {"fwd", "inv", "sandwich"};
+        int st = timer_mark(tm, s, std::string("xcol_kernel<f32,") + std::to_string(f.nx) + "," + mn[mode] + ">",
+                            (double)f.nx * ncols * 16.0);
+        if (st != FFTB_SUCCESS) return st;
+    }
+    float2 *d = (float2 *)data;
+    long long stride = ncols;
+    int nc = (int)ncols;
+    const float2 *rt = (const float2 *)f.roots_x;
+    void *args[] = {&d, &stride, &nc, &rt, &x};
+    const unsigned grid = (unsigned)((ncols + W - 1) / W);
+    return set_status_from_cuda(cudaLaunchKernel(e->fn[mode], dim3(grid), dim3(256), args, e->smem, s));
+}
+
+} // namespace
 
 int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz)
 {
@@ -11,21 +552,63 @@ int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz
     f.nx = nx;
     f.ny = ny;
     f.nz = nz;
+    if (dtype != FFTB_F32) return FFTB_SUCCESS;
+    if (getenv("FFTB_DISABLE_FUSED3D")) return FFTB_SUCCESS;
+    const PlaneEntry *pe = nullptr;
+    // one CTA per plane when it fits and the grid fills the GPU; otherwise a 2-CTA cluster
+    const PlaneEntry *p1 = find_plane(dtype, (int)ny, (int)nz, 1);
+    const PlaneEntry *p2 = find_plane(dtype, (int)ny, (int)nz, 2);
+    if (p1 && p1->smem_fwd <= 110 * 1024 && p1->smem_inv <= 110 * 1024 && nx >= 148) pe = p1;
+    else if (p2) pe = p2;
+    else if (p1) pe = p1;
+    const XColEntry *xe = find_xcol(dtype, (int)nx);
+    if (!pe || !xe) return FFTB_SUCCESS;
+    int st;
+    if ((st = configure(pe->fwd, pe->smem_fwd)) != FFTB_SUCCESS) return st;
+    if ((st = configure(pe->inv, pe->smem_inv)) != FFTB_SUCCESS) return st;
+    for (int m = 0; m < 3; ++m)
+        if ((st = configure(xe->fn[m], xe->smem)) != FFTB_SUCCESS) return st;
+    const int nmax = (int)(ny > nz ? ny : nz);
+    if ((st = engine_roots(dtype, nmax, &f.roots_plane)) != FFTB_SUCCESS) return st;
+    if ((st = engine_roots(dtype, (int)nx, &f.roots_x)) != FFTB_SUCCESS) return st;
+    f.plane = pe;
+    f.xcol = xe;
+    f.enabled = true;
     return FFTB_SUCCESS;
 }
 
-int fused3d_forward(const Fused3D &, const void *, void *, cudaStream_t, LaunchTimer *)
+int fused3d_forward(const Fused3D &f, const void *in, void *out, cudaStream_t s, LaunchTimer *t)
 {
-    return FFTB_ERROR_UNSUPPORTED_SIZE;
+    int st = launch_plane(f, false, in, out, 1.0, s, t);
+    if (st == FFTB_SUCCESS) st = launch_xcol(f, 0, out, nullptr, s, t);
+    if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
+    return st;
 }
-int fused3d_backward(const Fused3D &, void *, void *, double, cudaStream_t, LaunchTimer *)
+
+int fused3d_backward(const Fused3D &f, void *in, void *out, double scale, cudaStream_t s, LaunchTimer *t)
 {
-    return FFTB_ERROR_UNSUPPORTED_SIZE;
+    int st = launch_xcol(f, 1, in, nullptr, s, t);
+    if (st == FFTB_SUCCESS) st = launch_plane(f, true, in, out, scale, s, t);
+    if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
+    return st;
 }
-int fused3d_spectral(const Fused3D &, const void *, void *, void *, const EpValues &, cudaStream_t, LaunchTimer *)
+
+int fused3d_spectral(const Fused3D &f, const void *in, void *out, void *work, const EpValues &ep, cudaStream_t s,
+                     LaunchTimer *t)
 {
-    return FFTB_ERROR_UNSUPPORTED_SIZE;
+    if (!work) return FFTB_ERROR_NO_WORK_AREA;
+    int st = launch_plane(f, false, in, work, 1.0, s, t);
+    if (st == FFTB_SUCCESS) st = launch_xcol(f, 2, work, &ep, s, t);
+    if (st == FFTB_SUCCESS)
+        st = launch_plane(f, true, work, out, 1.0 / (double)(f.nx * f.ny * f.nz), s, t);
+    if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
+    return st;
 }
-int fused3d_num_launches(const Fused3D &, int) { return 0; }
+
+int fused3d_num_launches(const Fused3D &f, int which)
+{
+    (void)f;
+    return which <= 1 ? 2 : 3;
+}
 
 } // namespace fftb

@@ -12,7 +12,10 @@ struct Fused3D {
     bool enabled = false;
     int dtype = 0;
     long long nx = 0, ny = 0, nz = 0;
-    Program xfwd, xinv, xsand;  // generic x-axis passes used between the fused kernels
+    const void *plane = nullptr;   // selected plane kernel entry
+    const void *xcol = nullptr;    // selected x column kernel entry
+    void *roots_plane = nullptr;   // device root table of length max(ny, nz)
+    void *roots_x = nullptr;       // device root table of length nx
 };
 
 // Sets f.enabled when (dtype, nx, ny, nz) has a specialised path.

@@ -1,0 +1,80 @@
+// fftb_regfft.cuh -- register-resident two-stage FFTs for the specialised kernels.
+//
+// An N-point FFT (N = 16*T, T in {1, 2, 4, 8, 16}) is run by T threads, each
+// holding 16 complex values.  Thread t starts with v[r] = x[t + T*r] and ends
+// with v[j] = X[t + T*j]:
+//   stage 1: radix-16 DFT over r in registers        -> Y_t[k1]
+//   twiddle: Y_t[k1] *= w_N^(t*k1)
+//   exchange through this FFT's shared-memory region  (one store, one load)
+//   stage 2: 16/T DFTs of length T over t in registers -> X[k1 + 16*k2]
+// (the four-step decomposition X[k1 + 16 k2] = sum_t w_T^(t k2) w_N^(t k1)
+//  sum_r x[t + T r] w_16^(r k1)).
+#pragma once
+
+#include "fftb_device.cuh"
+
+namespace fftb {
+
+// Size of one FFT's exchange region (complex entries).  Regions of the FFTs that
+// share a half-warp are offset by T (mod 16) so stores and loads are conflict-free.
+template <int N> struct RegFFTShape {
+    static constexpr int T = N >= 16 ? N / 16 : 1;
+    static constexpr int ROWP = T + 1;                         // entries per k1 row
+    static constexpr int REGION = (T == 1) ? 16 : 16 * ROWP + (T == 16 ? 0 : T);
+};
+
+template <int SIGN, int L, typename C, typename R> __device__ __forceinline__ void dft_small(C *u)
+{
+    if constexpr (L == 1) {
+    } else if constexpr (L == 2) {
+        dft2<SIGN>(u[0], u[1]);
+    } else if constexpr (L == 4) {
+        dft4<SIGN>(u[0], u[1], u[2], u[3]);
+    } else if constexpr (L == 8) {
+        dft8<SIGN, C, R>(u);
+    } else {
+        static_assert(L == 16, "length");
+        dft16<SIGN, C, R>(u);
+    }
+}
+
+// Multiplies v by w^e (SIGN<0) or conj(w)^e (SIGN>0) with w^e = tw[e*stride].
+template <int SIGN, typename C> __device__ __forceinline__ C twiddle_mul(C v, const C *tw, int idx)
+{
+    const C w = tw[idx];
+    return SIGN < 0 ? cmul(v, w) : cmulc(v, w);
+}
+
+// SYNC: 0 = the T threads of this FFT are in one warp (__syncwarp),
+//       1 = they span warps (__syncthreads; every thread of the block must call).
+// reg: exchange region; for SYNC==1 the caller passes a layout functor instead.
+template <typename R, int N, int SIGN>
+__device__ __forceinline__ void regfft_warp(cpx<R> (&v)[16], cpx<R> *reg, const cpx<R> *tw, int tws, int t)
+{
+    using C = cpx<R>;
+    using S = RegFFTShape<N>;
+    constexpr int T = S::T;
+    if constexpr (N <= 16) {
+        dft_small<SIGN, N, C, R>(v);
+    } else {
+        dft16<SIGN, C, R>(v);
+#pragma unroll
+        for (int k1 = 1; k1 < 16; ++k1) v[k1] = twiddle_mul<SIGN>(v[k1], tw, t * k1 * tws);
+        __syncwarp();
+#pragma unroll
+        for (int k1 = 0; k1 < 16; ++k1) reg[k1 * S::ROWP + t] = v[k1];
+        __syncwarp();
+        constexpr int A = 16 / T;
+#pragma unroll
+        for (int a = 0; a < A; ++a) {
+            C u[T];
+#pragma unroll
+            for (int q = 0; q < T; ++q) u[q] = reg[(t + T * a) * S::ROWP + q];
+            dft_small<SIGN, T, C, R>(u);
+#pragma unroll
+            for (int k2 = 0; k2 < T; ++k2) v[a + A * k2] = u[k2];
+        }
+    }
+}
+
+} // namespace fftb

@@ -1,0 +1,106 @@
+"""GPU parity of the specialised fused 3D path (plane kernels with and without a
+2-CTA cluster, x column kernels) against the FP64 oracle, f32 tolerance 2e-6."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 2e-6
+
+# (nx, ny, nz): sizes with a specialised path; the comment names the plane variant chosen
+FUSED = [
+    (64, 64, 64),      # 2-CTA cluster (nx < 148)
+    (256, 64, 64),     # one CTA per plane
+    (32, 128, 256),    # cluster, nx = 32
+    (64, 256, 128),    # cluster
+    (128, 128, 128),   # cluster
+    (256, 128, 64),    # one CTA per plane
+    (256, 256, 256),   # cluster, the benchmark size
+]
+
+
+@pytest.fixture(scope="module")
+def F(torch_cuda):
+    from fftm_b200 import build
+    build.build()
+    import fftm_b200
+    return fftm_b200
+
+
+def _dev(torch, a):
+    return torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device="cuda")
+
+
+def _host(t):
+    import torch
+    torch.cuda.synchronize()
+    return t.cpu().numpy().astype(np.complex128 if t.is_complex() else np.float64)
+
+
+@pytest.mark.parametrize("shape", FUSED)
+def test_fused_forward_backward(F, torch_cuda, shape):
+    torch = torch_cuda
+    f = F.ffts("float32").init(*shape)
+    assert f.num_launches("forward") == 2 and f.num_launches("poisson") == 3
+    x = O.random_3d(*shape, 0x1234ABCDEF987654, single=True)
+    xin = _dev(torch, x)
+    spec = torch.empty(f.spectrum_shape(), dtype=torch.complex64, device="cuda")
+    f.forward(xin, spec)
+    ref = O.ffts3d_forward(x)
+    assert O.rel_l2(_host(spec), ref) <= TOL
+    out = torch.empty_like(xin)
+    f.backward(spec, out)
+    assert O.rel_l2(_host(out) / x.size, x) <= TOL
+    spec2 = torch.tensor(ref, dtype=torch.complex64, device="cuda")
+    f.backward(spec2, out, normalized=True)
+    assert O.rel_l2(_host(out), x) <= TOL
+
+
+@pytest.mark.parametrize("shape", FUSED)
+def test_fused_poisson_and_filter(F, torch_cuda, shape):
+    torch = torch_cuda
+    f = F.ffts("float32").init(*shape)
+    rhs = O.random_3d(*shape, 99, single=True)
+    sol = torch.empty(shape, dtype=torch.float32, device="cuda")
+    f.poisson(_dev(torch, rhs), sol, -1.0)
+    assert O.rel_l2(_host(sol), O.poisson3d_solve(rhs, -1.0)) <= TOL
+    f.poisson(_dev(torch, rhs), sol, +1.0)
+    assert O.rel_l2(_host(sol), O.poisson3d_solve(rhs, +1.0)) <= TOL
+    sigma = 6.0
+    f.filter(_dev(torch, rhs), sol, sigma, poisson_sign=-1.0)
+    X = O.ffts3d_forward(rhs)
+    nx, ny, nz = shape
+    kx = np.fft.fftfreq(nx, 1.0 / nx)[:, None, None]
+    ky = np.fft.fftfreq(ny, 1.0 / ny)[None, :, None]
+    kz = np.arange(nz // 2 + 1)[None, None, :]
+    k2 = kx ** 2 + ky ** 2 + kz ** 2
+    with np.errstate(divide="ignore", invalid="ignore"):
+        P = np.where(k2 == 0, 0.0, -1.0 / k2)
+    ref = O.ffts3d_backward(X * np.exp(-k2 / (2 * sigma ** 2)) * P, nz) / rhs.size
+    assert O.rel_l2(_host(sol), ref) <= TOL
+
+
+def test_fused_poisson_manufactured_256(F, torch_cuda):
+    torch = torch_cuda
+    n = 256
+    g = 2 * np.pi * np.arange(n) / n
+    u = (np.sin(g)[:, None, None] * np.cos(2 * g)[None, :, None] * np.sin(3 * g)[None, None, :])
+    f = F.ffts("float32").init(n, n, n)
+    sol = torch.empty((n, n, n), dtype=torch.float32, device="cuda")
+    f.poisson(_dev(torch, 14 * u), sol, +1.0)
+    assert O.rel_l2(_host(sol), u) <= TOL
+
+
+def test_fused_round_trip_criterion_256(F, torch_cuda):
+    # the reference benchmarks' pin: RMS(C2R(R2C(x))/N - x) <= 10 eps_f32
+    torch = torch_cuda
+    shape = (256, 256, 256)
+    f = F.ffts("float32").init(*shape)
+    x = torch.rand(shape, device="cuda") * 2 - 1
+    spec = torch.empty(f.spectrum_shape(), dtype=torch.complex64, device="cuda")
+    out = torch.empty_like(x)
+    f.forward(x, spec)
+    f.backward(spec, out, normalized=True)
+    rms = torch.sqrt(torch.mean((out - x) ** 2)).item()
+    assert rms <= 10 * np.finfo(np.float32).eps
