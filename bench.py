@@ -331,6 +331,39 @@ def main():
         e2e_ms = float(t.item())
     e2e_val = BYTES_RT * e2e_steps * world / (e2e_ms * 1e-3) / 1e9
 
+    # the same solve through cuFFT (torch.fft: R2C, multiply by -1/|k|^2, C2R with 1/N), the
+    # library the reference's ffts wraps, timed with the same flush / event protocol
+    cufft = None
+    try:
+        kx = torch.fft.fftfreq(NX, 1.0 / NX, device=dev)[:, None, None]
+        ky = torch.fft.fftfreq(NY, 1.0 / NY, device=dev)[None, :, None]
+        kz = torch.arange(NZ // 2 + 1, device=dev, dtype=torch.float32)[None, None, :]
+        k2 = kx * kx + ky * ky + kz * kz
+        mult = torch.where(k2 == 0, torch.zeros_like(k2), -1.0 / k2).to(torch.float32)
+
+        def cufft_step():
+            X = torch.fft.rfftn(rhs)
+            X.mul_(mult)
+            return torch.fft.irfftn(X, s=(NX, NY, NZ))
+
+        for _ in range(3):
+            flush.zero_()
+            cufft_step()
+        torch.cuda.synchronize()
+        cs = [torch.cuda.Event(enable_timing=True) for _ in range(20)]
+        ce = [torch.cuda.Event(enable_timing=True) for _ in range(20)]
+        for i in range(20):
+            flush.zero_()
+            cs[i].record(stream)
+            cufft_step()
+            ce[i].record(stream)
+        torch.cuda.synchronize()
+        cms = sum(a.elapsed_time(b) for a, b in zip(cs, ce)) / 20
+        cufft = {"impl": "torch.fft (cuFFT) rfftn, multiply, irfftn", "ms_per_step": cms,
+                 "value": BYTES_RT / (cms * 1e-3) / 1e9, "unit": "GB/s"}
+    except Exception as exc:  # noqa: BLE001
+        cufft = {"unavailable": str(exc)[:200]}
+
     # accuracy of the timed solution against the analytic solution of the smooth part is not
     # defined (the noise term has no closed form); the CPU leg checks it against the FP64 oracle.
     result = sol.detach().cpu().numpy()
@@ -350,6 +383,7 @@ def main():
                 "d2h_bytes_per_step": int(sol.numel() * 4), "steps": e2e_steps,
                 "ms_per_step": e2e_ms / e2e_steps},
         "clocks": clk,
+        "cufft_same_gpu": cufft,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, secs, threads, ref = cpu_oracle_rate(f_host, 1)

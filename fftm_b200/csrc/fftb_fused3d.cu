@@ -33,7 +33,7 @@ namespace cg = cooperative_groups;
 namespace fftb {
 
 // ------------------------------------------------------------------ plane kernels
-// Work split (CL CTAs per plane, CL in {1, 2}):
+// Work split (CL CTAs per plane, CL in {1, 2, 4}):
 //   rows   : CTA c owns rows [c*M, (c+1)*M) for the z stage            (M = NY / CL)
 //   columns: CTA c owns column slots [c*S, (c+1)*S) for the y stage     (S = NZ / (2 CL))
 // Slot s < NZ/2 is spectrum column kz = s, except slot 0, which packs the two
@@ -44,7 +44,7 @@ namespace fftb {
 // between the stages is pushed with distributed-shared-memory stores, so no CTA
 // ever reads another CTA's shared memory.
 template <int NY, int NZ, int CL> struct PlaneShape {
-    static constexpr int NT = CL > 1 ? 512 : 256;            // threads per CTA
+    static constexpr int NT = 256;                           // threads per CTA
     static constexpr int M = NY / CL;                        // rows per CTA (z stage)
     static constexpr int S = NZ / (2 * CL);                  // column slots per CTA (y stage)
     static constexpr int NS = NZ / 2;                        // slots of the plane
@@ -52,6 +52,7 @@ template <int NY, int NZ, int CL> struct PlaneShape {
     static constexpr int TY = RegFFTShape<NY>::T;
     static constexpr int FZ = NT / TZ, FY = NT / TY;         // concurrent FFTs per stage
     static constexpr int NMAX = NY > NZ ? NY : NZ;
+    static constexpr int TWS = NY + NZ;                      // stage tables of the z and y FFTs
     // forward: y-stage plane [NY][PF], PF = 16/TY (mod 16) -> conflict-free column reads
     static constexpr int PMOD = 16 / TY;
     static constexpr int PF = S + ((PMOD - S % 16) % 16 + 16) % 16;
@@ -59,18 +60,19 @@ template <int NY, int NZ, int CL> struct PlaneShape {
     static constexpr int SCR_Y = FY * RegFFTShape<NY>::REGION;
     static constexpr int SCRF = SCR_Z > SCR_Y ? SCR_Z : SCR_Y;
     // inverse: z-stage rows [M][PR] (PR odd -> conflict-free column pushes) and a
-    // column-major staging area of FY columns of PC entries (PC odd, >= REGION)
+    // column-major staging area of FY columns of PC entries (PC odd, >= REGION) that
+    // also serves as the FFT exchange regions
     static constexpr int PR = NS + 1;
     static constexpr int REGY = RegFFTShape<NY>::REGION > NY ? RegFFTShape<NY>::REGION : NY;
     static constexpr int PC = REGY | 1;
     static constexpr int STG = FY * PC > SCR_Z ? FY * PC : SCR_Z;
     template <typename R> static constexpr size_t smem_fwd()
     {
-        return sizeof(cpx<R>) * ((size_t)NY * PF + SCRF + NMAX);
+        return sizeof(cpx<R>) * ((size_t)NY * PF + SCRF + TWS);
     }
     template <typename R> static constexpr size_t smem_inv()
     {
-        return sizeof(cpx<R>) * ((size_t)M * PR + STG + NMAX);
+        return sizeof(cpx<R>) * ((size_t)M * PR + STG + TWS);
     }
 };
 
@@ -83,16 +85,20 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *plane = reinterpret_cast<C *>(smem_raw);   // [NY][PF]: this CTA's column slots
     C *scr = plane + NY * S::PF;
-    C *tw = scr + S::SCRF;
+    C *twz = scr + S::SCRF;                       // stage table of the z FFT
+    C *twy = twz + NZ;                            // stage table of the y FFT
     const int tid = threadIdx.x;
     const int c = (CL > 1) ? (int)cg::this_cluster().block_rank() : 0;
     const int x = (int)(blockIdx.x / CL);
-    C *dst[2] = {plane, plane};
+    C *dst[CL];
+#pragma unroll
+    for (int q = 0; q < CL; ++q) dst[q] = plane;
     if constexpr (CL > 1) {
-        dst[0] = cg::this_cluster().map_shared_rank(plane, 0u);
-        dst[1] = cg::this_cluster().map_shared_rank(plane, 1u);
+#pragma unroll
+        for (int q = 0; q < CL; ++q) dst[q] = cg::this_cluster().map_shared_rank(plane, (unsigned)q);
     }
-    for (int i = tid; i < S::NMAX; i += S::NT) tw[i] = roots[i];
+    build_stage_table<R, NZ>(twz, roots, S::NMAX, tid, S::NT);
+    build_stage_table<R, NY>(twy, roots, S::NMAX, tid, S::NT);
     __syncthreads();
 
     // ---- stage z: R2C of this CTA's rows (two rows per complex FFT), pushed to the slot owners
@@ -114,28 +120,35 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT)
                 v[r].x = ra[t + TZ * r];
                 v[r].y = rb[t + TZ * r];
             }
-            regfft_warp<R, NZ, -1>(v, reg, tw, S::NMAX / NZ, t);
-            __syncwarp();
+            regfft_warp<R, NZ, -1>(v, reg, twz, t);
+            // separate the two real rows with Z[-k] fetched from the partner lane:
+            // Z[t + TZ j] sits in lane t, register j; Z[NZ - (t + TZ j)] in lane (TZ - t) mod TZ,
+            // register 15 - j (t > 0) or in this lane, register (16 - j) mod 16 (t = 0)
+            const int lane = threadIdx.x & 31;
+            const int src = (lane - t) + ((TZ - t) & (TZ - 1));
+            // every lane runs the shuffles (groups of one warp may differ in `ok`)
+            const int ya = c * S::M + 2 * pp;  // row index within the plane
+            const C zn = mk<R>(__shfl_sync(0xffffffffu, v[8].x, lane - t),
+                               __shfl_sync(0xffffffffu, v[8].y, lane - t));  // Z[NZ/2]: lane t=0, j=8
 #pragma unroll
-            for (int j = 0; j < 16; ++j) reg[t + TZ * j] = v[j];
-            __syncwarp();
-            if (ok) {
-                const int ya = c * S::M + 2 * pp;  // row index within the plane
-#pragma unroll
-                for (int j = 0; j < NZ / (2 * TZ); ++j) {
-                    const int k = t + TZ * j;      // k < NZ/2
-                    const C zk = reg[k];
-                    const C zm = cconj(reg[(NZ - k) & (NZ - 1)]);
-                    C A = cscale(cadd(zk, zm), R(0.5));
-                    C B = cscale(mul_si<-1>(csub(zk, zm)), R(0.5));
-                    if (k == 0) {
-                        // pack kz = 0 (real) and kz = NZ/2 (real) into slot 0
-                        const C zn = reg[NZ / 2];
-                        A = mk<R>(zk.x, zn.x);
-                        B = mk<R>(zk.y, zn.y);
-                    }
+            for (int j = 0; j < NZ / (2 * TZ); ++j) {
+                const int k = t + TZ * j;      // k < NZ/2
+                const C zk = v[j];
+                C zp;
+                zp.x = __shfl_sync(0xffffffffu, v[15 - j].x, src);
+                zp.y = __shfl_sync(0xffffffffu, v[15 - j].y, src);
+                if (t == 0) zp = v[(16 - j) & 15];
+                const C zm = cconj(zp);
+                C A = cscale(cadd(zk, zm), R(0.5));
+                C B = cscale(mul_si<-1>(csub(zk, zm)), R(0.5));
+                if (k == 0) {
+                    // pack kz = 0 (real) and kz = NZ/2 (real) into slot 0
+                    A = mk<R>(zk.x, zn.x);
+                    B = mk<R>(zk.y, zn.y);
+                }
+                if (ok) {
                     const int owner = k / S::S, ls = k - owner * S::S;
-                    C *d = dst[CL > 1 ? owner : 0];
+                    C *d = dst[owner];
                     d[ya * S::PF + ls] = A;
                     d[(ya + 1) * S::PF + ls] = B;
                 }
@@ -160,27 +173,30 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT)
             C v[16];
 #pragma unroll
             for (int r = 0; r < 16; ++r) v[r] = plane[(t + TY * r) * S::PF + slc];
-            regfft_warp<R, NY, -1>(v, reg, tw, S::NMAX / NY, t);
-            // the packed slot: X0[ky] = (W[ky] + conj W[-ky]) / 2, XN[ky] = (W[ky] - conj W[-ky]) / 2i
-            __syncwarp();
+            regfft_warp<R, NY, -1>(v, reg, twy, t);
+            // the packed slot (slot 0 of CTA 0, first round, warp 0):
+            // X0[ky] = (W[ky] + conj W[-ky]) / 2, XN[ky] = (W[ky] - conj W[-ky]) / 2i
+            if (c == 0 && s0 == 0 && (tid >> 5) == 0) {
+                __syncwarp();
 #pragma unroll
-            for (int j = 0; j < 16; ++j) reg[t + TY * j] = v[j];
-            __syncwarp();
-            if (ok && c == 0 && sl == 0) {
+                for (int j = 0; j < 16; ++j) reg[t + TY * j] = v[j];
+                __syncwarp();
+                if (sl == 0) {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int ky = t + TY * j;
-                    const C wk = v[j];
-                    const C wm = cconj(reg[(NY - ky) & (NY - 1)]);
-                    v[j] = cscale(cadd(wk, wm), R(0.5));
-                    oplane[(size_t)ky * (NZ / 2 + 1) + NZ / 2] = cscale(mul_si<-1>(csub(wk, wm)), R(0.5));
+                    for (int j = 0; j < 16; ++j) {
+                        const int ky = t + TY * j;
+                        const C wk = v[j];
+                        const C wm = cconj(reg[(NY - ky) & (NY - 1)]);
+                        v[j] = cscale(cadd(wk, wm), R(0.5));
+                        oplane[(size_t)ky * (NZ / 2 + 1) + NZ / 2] = cscale(mul_si<-1>(csub(wk, wm)), R(0.5));
+                    }
                 }
+                __syncwarp();
             }
             if (ok) {
 #pragma unroll
                 for (int j = 0; j < 16; ++j) plane[(t + TY * j) * S::PF + slc] = v[j];
             }
-            __syncwarp();
         }
     }
     __syncthreads();
@@ -203,17 +219,22 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT)
     using S = PlaneShape<NY, NZ, CL>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *rowsm = reinterpret_cast<C *>(smem_raw);   // [M][PR]: this CTA's rows, every slot
-    C *stg = rowsm + S::M * S::PR;                // staging columns / FFT exchange regions
-    C *tw = stg + S::STG;
+    C *stg = rowsm + S::M * S::PR;                // FFT exchange regions
+    C *twz = stg + S::STG;
+    C *twy = twz + NZ;
     const int tid = threadIdx.x;
     const int c = (CL > 1) ? (int)cg::this_cluster().block_rank() : 0;
     const int x = (int)(blockIdx.x / CL);
-    C *dst[2] = {rowsm, rowsm};
+    C *dst[CL];
+#pragma unroll
+    for (int q = 0; q < CL; ++q) dst[q] = rowsm;
     if constexpr (CL > 1) {
-        dst[0] = cg::this_cluster().map_shared_rank(rowsm, 0u);
-        dst[1] = cg::this_cluster().map_shared_rank(rowsm, 1u);
+#pragma unroll
+        for (int q = 0; q < CL; ++q) dst[q] = cg::this_cluster().map_shared_rank(rowsm, (unsigned)q);
     }
-    for (int i = tid; i < S::NMAX; i += S::NT) tw[i] = roots[i];
+    build_stage_table<R, NZ>(twz, roots, S::NMAX, tid, S::NT);
+    build_stage_table<R, NY>(twy, roots, S::NMAX, tid, S::NT);
+    __syncthreads();
     const C *iplane = in + (size_t)x * NY * (NZ / 2 + 1);
 
     // ---- stage y: inverse FFT of the owned slots, rows pushed to their owners
@@ -245,17 +266,16 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT)
                     v[r] = mk<R>(v[r].x - xn.y, v[r].y + xn.x);
                 }
             }
+            regfft_warp<R, NY, +1>(v, col, twy, t);
+            // back into the staging column, then push whole row segments to the row owners
             __syncwarp();
-            regfft_warp<R, NY, +1>(v, col, tw, S::NMAX / NY, t);
-            if (ok) {
-                const int gs = c * S::S + sl;
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int m = t + TY * j;
-                    const int owner = m / S::M;
-                    C *d = dst[CL > 1 ? owner : 0];
-                    d[(m - owner * S::M) * S::PR + gs] = v[j];
-                }
+            for (int j = 0; j < 16; ++j) col[t + TY * j] = v[j];
+            __syncthreads();
+            for (int e = tid; e < NY * ns; e += S::NT) {
+                const int m = e / ns, q = e - (e / ns) * ns;
+                const int owner = m / S::M;
+                dst[owner][(m - owner * S::M) * S::PR + c * S::S + s0 + q] = stg[q * S::PC + m];
             }
             __syncthreads();  // the staging area is reused by the next round
         }
@@ -295,7 +315,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT)
                 }
                 v[r] = mk<R>(ha.x - hb.y, ha.y + hb.x);  // Ha + i Hb
             }
-            regfft_warp<R, NZ, +1>(v, reg, tw, S::NMAX / NZ, t);
+            regfft_warp<R, NZ, +1>(v, reg, twz, t);
             if (ok) {
                 R *ra = rows + (size_t)(2 * pp) * NZ;
                 R *rb = ra + NZ;
@@ -352,7 +372,7 @@ __device__ __forceinline__ void xcol_fft(cpx<R> (&v)[16], cpx<R> *scr, const cpx
 }
 
 template <typename R, int NX, int MODE>  // MODE 0: forward, 1: inverse, 2: forward-multiply-inverse
-__global__ void __launch_bounds__(256) xcol_kernel(cpx<R> *__restrict__ data, long long stride, int ncols,
+__global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data, long long stride, int ncols,
                                                    const cpx<R> *__restrict__ roots, XColEp ep)
 {
     using C = cpx<R>;
@@ -377,18 +397,31 @@ __global__ void __launch_bounds__(256) xcol_kernel(cpx<R> *__restrict__ data, lo
         const int ky_i = cg0 / ep.nzh, kz = cg0 - (cg0 / ep.nzh) * ep.nzh;
         const int ky = ky_i <= ep.ny / 2 ? ky_i : ky_i - ep.ny;
         const R kyz = R(ky * ky + kz * kz);
+        const R sc = sizeof(R) == 4 ? R(ep.scale_f) : R(ep.scale);
+        const R sg = sizeof(R) == 4 ? R(ep.sign_f) : R(ep.sign);
+        if ((ep.mode & (EP_POISSON | EP_GAUSS)) == EP_POISSON) {
+            const R ss = sc * sg;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const int kxi = t + T * j;
-            const int kx = kxi <= NX / 2 ? kxi : kxi - NX;
-            const R k2 = R(kx * kx) + kyz;
-            R fct = sizeof(R) == 4 ? R(ep.scale_f) : R(ep.scale);
-            if (ep.mode & EP_POISSON) {
-                const R sg = sizeof(R) == 4 ? R(ep.sign_f) : R(ep.sign);
-                fct = (k2 == R(0)) ? R(0) : fct * sg / k2;
+            for (int j = 0; j < 16; ++j) {
+                const int kxi = t + T * j;
+                const int kx = kxi <= NX / 2 ? kxi : kxi - NX;
+                const R k2 = R(kx * kx) + kyz;
+                R inv;
+                if constexpr (sizeof(R) == 4) inv = __frcp_rn(k2);
+                else inv = R(1) / k2;
+                v[j] = cscale(v[j], (k2 == R(0)) ? R(0) : ss * inv);
             }
-            if (ep.mode & EP_GAUSS) fct *= exp(-k2 * (sizeof(R) == 4 ? R(ep.gauss_f) : R(ep.gauss)));
-            v[j] = cscale(v[j], fct);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int kxi = t + T * j;
+                const int kx = kxi <= NX / 2 ? kxi : kxi - NX;
+                const R k2 = R(kx * kx) + kyz;
+                R fct = sc;
+                if (ep.mode & EP_POISSON) fct = (k2 == R(0)) ? R(0) : fct * sg / k2;
+                if (ep.mode & EP_GAUSS) fct *= exp(-k2 * (sizeof(R) == 4 ? R(ep.gauss_f) : R(ep.gauss)));
+                v[j] = cscale(v[j], fct);
+            }
         }
         xcol_fft<R, NX, +1>(v, scr, tw, t, col);
     }
@@ -415,13 +448,12 @@ template <typename R, int NY, int NZ, int CL> PlaneEntry plane_entry(int dtype)
                       S::template smem_inv<R>()};
 }
 
+#define FFTB_PLANE3(R, D, NY, NZ)                                                                                   \
+    plane_entry<R, NY, NZ, 1>(D), plane_entry<R, NY, NZ, 2>(D), plane_entry<R, NY, NZ, 4>(D)
 #define FFTB_PLANES(R, D)                                                                                          \
-    plane_entry<R, 64, 64, 1>(D), plane_entry<R, 64, 64, 2>(D), plane_entry<R, 64, 128, 1>(D),                    \
-        plane_entry<R, 64, 128, 2>(D), plane_entry<R, 64, 256, 1>(D), plane_entry<R, 64, 256, 2>(D),              \
-        plane_entry<R, 128, 64, 1>(D), plane_entry<R, 128, 64, 2>(D), plane_entry<R, 128, 128, 1>(D),             \
-        plane_entry<R, 128, 128, 2>(D), plane_entry<R, 128, 256, 1>(D), plane_entry<R, 128, 256, 2>(D),           \
-        plane_entry<R, 256, 64, 1>(D), plane_entry<R, 256, 64, 2>(D), plane_entry<R, 256, 128, 1>(D),             \
-        plane_entry<R, 256, 128, 2>(D), plane_entry<R, 256, 256, 2>(D)
+    FFTB_PLANE3(R, D, 64, 64), FFTB_PLANE3(R, D, 64, 128), FFTB_PLANE3(R, D, 64, 256), FFTB_PLANE3(R, D, 128, 64), \
+        FFTB_PLANE3(R, D, 128, 128), FFTB_PLANE3(R, D, 128, 256), FFTB_PLANE3(R, D, 256, 64),                     \
+        FFTB_PLANE3(R, D, 256, 128), FFTB_PLANE3(R, D, 256, 256)
 
 const PlaneEntry *find_plane(int dtype, int ny, int nz, int cl)
 {
@@ -554,13 +586,21 @@ int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz
     f.nz = nz;
     if (dtype != FFTB_F32) return FFTB_SUCCESS;
     if (getenv("FFTB_DISABLE_FUSED3D")) return FFTB_SUCCESS;
+    // the smallest cluster whose CTAs fit two per SM and whose grid fills two waves;
+    // failing that, the smallest one that fits one per SM
     const PlaneEntry *pe = nullptr;
-    // one CTA per plane when it fits and the grid fills the GPU; otherwise a 2-CTA cluster
-    const PlaneEntry *p1 = find_plane(dtype, (int)ny, (int)nz, 1);
-    const PlaneEntry *p2 = find_plane(dtype, (int)ny, (int)nz, 2);
-    if (p1 && p1->smem_fwd <= 110 * 1024 && p1->smem_inv <= 110 * 1024 && nx >= 148) pe = p1;
-    else if (p2) pe = p2;
-    else if (p1) pe = p1;
+    for (int cl = 1; cl <= 4 && !pe; cl *= 2) {
+        const PlaneEntry *e = find_plane(dtype, (int)ny, (int)nz, cl);
+        if (e && e->smem_fwd <= 113 * 1024 && e->smem_inv <= 113 * 1024 && nx * cl >= 2 * 148) pe = e;
+    }
+    for (int cl = 4; cl >= 1 && !pe; cl /= 2) {
+        const PlaneEntry *e = find_plane(dtype, (int)ny, (int)nz, cl);
+        if (e && e->smem_fwd <= 113 * 1024 && e->smem_inv <= 113 * 1024) pe = e;
+    }
+    for (int cl = 1; cl <= 4 && !pe; cl *= 2) {
+        const PlaneEntry *e = find_plane(dtype, (int)ny, (int)nz, cl);
+        if (e && e->smem_fwd <= 227 * 1024 && e->smem_inv <= 227 * 1024) pe = e;
+    }
     const XColEntry *xe = find_xcol(dtype, (int)nx);
     if (!pe || !xe) return FFTB_SUCCESS;
     int st;

@@ -45,11 +45,22 @@ template <int SIGN, typename C> __device__ __forceinline__ C twiddle_mul(C v, co
     return SIGN < 0 ? cmul(v, w) : cmulc(v, w);
 }
 
-// SYNC: 0 = the T threads of this FFT are in one warp (__syncwarp),
-//       1 = they span warps (__syncthreads; every thread of the block must call).
-// reg: exchange region; for SYNC==1 the caller passes a layout functor instead.
+// Stage twiddle table of an N-point register FFT: st[k1 * T + t] = w_N^(t * k1), so the
+// 16 twiddle loads of the T threads of one FFT hit consecutive shared-memory words.
+template <typename R, int N>
+__device__ __forceinline__ void build_stage_table(cpx<R> *st, const cpx<R> *roots, int nroots, int tid, int nthreads)
+{
+    constexpr int T = RegFFTShape<N>::T;
+    for (int i = tid; i < 16 * T; i += nthreads) {
+        const int k1 = i / T, t = i - (i / T) * T;
+        st[i] = roots[((t * k1) % N) * (nroots / N)];
+    }
+}
+
+// The T threads of this FFT must be consecutive lanes of one warp (exchange with
+// __syncwarp).  st: stage table of build_stage_table<R, N>; reg: exchange region.
 template <typename R, int N, int SIGN>
-__device__ __forceinline__ void regfft_warp(cpx<R> (&v)[16], cpx<R> *reg, const cpx<R> *tw, int tws, int t)
+__device__ __forceinline__ void regfft_warp(cpx<R> (&v)[16], cpx<R> *reg, const cpx<R> *st, int t)
 {
     using C = cpx<R>;
     using S = RegFFTShape<N>;
@@ -59,7 +70,7 @@ __device__ __forceinline__ void regfft_warp(cpx<R> (&v)[16], cpx<R> *reg, const 
     } else {
         dft16<SIGN, C, R>(v);
 #pragma unroll
-        for (int k1 = 1; k1 < 16; ++k1) v[k1] = twiddle_mul<SIGN>(v[k1], tw, t * k1 * tws);
+        for (int k1 = 1; k1 < 16; ++k1) v[k1] = twiddle_mul<SIGN>(v[k1], st, k1 * T + t);
         __syncwarp();
 #pragma unroll
         for (int k1 = 0; k1 < 16; ++k1) reg[k1 * S::ROWP + t] = v[k1];
