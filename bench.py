@@ -331,6 +331,60 @@ def main():
         e2e_ms = float(t.item())
     e2e_val = BYTES_RT * e2e_steps * world / (e2e_ms * 1e-3) / 1e9
 
+    # secondary size of the metric: 4D 64^4 native_xzwy R2C + C2R round trip (forward, then the
+    # normalised inverse), input N(0,1) from default_rng(1), same flush / event protocol
+    sec = None
+    try:
+        d4 = (64, 64, 64, 64)
+        f4 = F.ffts("float32", strategy_4d="native_xzwy").init(*d4)
+        w4 = torch.empty(f4.work_size // 8 + 1, dtype=torch.complex64, device=dev)
+        f4.set_work_area(w4)
+        x4 = torch.from_numpy(np.random.default_rng(1).standard_normal(d4).astype(np.float32)).to(dev)
+        y4 = torch.empty_like(x4)
+        s4 = torch.empty(f4.spectrum_shape(), dtype=torch.complex64, device=dev)
+
+        def rt4():
+            f4.forward(x4, s4)
+            f4.backward(s4, y4, normalized=True)
+
+        for _ in range(3):
+            flush.zero_()
+            rt4()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(20)]
+        for a, b in ev:
+            flush.zero_()
+            a.record(stream)
+            rt4()
+            b.record(stream)
+        torch.cuda.synchronize()
+        ms4 = sum(a.elapsed_time(b) for a, b in ev) / len(ev)
+        b4 = 2 * (4 * 64 ** 4 + 8 * 64 ** 3 * 33)
+        err4 = float(torch.linalg.norm(y4 - x4) / torch.linalg.norm(x4))
+
+        def cufft4():
+            torch.fft.irfftn(torch.fft.rfftn(x4), s=d4)
+
+        for _ in range(3):
+            cufft4()
+        torch.cuda.synchronize()
+        cv = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(20)]
+        for a, b in cv:
+            flush.zero_()
+            a.record(stream)
+            cufft4()
+            b.record(stream)
+        torch.cuda.synchronize()
+        cms4 = sum(a.elapsed_time(b) for a, b in cv) / len(cv)
+        sec = {"workload": "4D 64^4 f32 native_xzwy R2C + normalised C2R round trip", "ms_per_step": ms4,
+               "value": b4 / (ms4 * 1e-3) / 1e9, "unit": "GB/s", "bytes_per_step": b4,
+               "launches_per_step": f4.num_launches("forward") + f4.num_launches("backward"),
+               "round_trip_rel_l2": err4,
+               "cufft_same_gpu": {"impl": "torch.fft rfftn + irfftn", "ms_per_step": cms4,
+                                  "value": b4 / (cms4 * 1e-3) / 1e9}}
+    except Exception as exc:  # noqa: BLE001
+        sec = {"unavailable": str(exc)[:200]}
+
     # the same solve through cuFFT (torch.fft: R2C, multiply by -1/|k|^2, C2R with 1/N), the
     # library the reference's ffts wraps, timed with the same flush / event protocol
     cufft = None
@@ -384,6 +438,7 @@ def main():
                 "ms_per_step": e2e_ms / e2e_steps},
         "clocks": clk,
         "cufft_same_gpu": cufft,
+        "secondary": sec,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, secs, threads, ref = cpu_oracle_rate(f_host, 1)

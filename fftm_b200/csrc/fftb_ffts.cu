@@ -26,7 +26,8 @@ struct fftb_ffts_s {
     void *work = nullptr;
     bool own_work = false;
     cudaStream_t stream = 0;
-    Fused3D fused;  // specialised 3D kernels (when the size has them)
+    Fused3D fused;   // specialised 3D kernels (when the size has them)
+    Fused4D fused4;  // specialised 4D slab / native_xzwy kernels
     LaunchTimer timer;
     bool timing = false;
 };
@@ -259,6 +260,8 @@ int build_4d(fftb_ffts_s *o)
     return FFTB_SUCCESS;
 }
 
+bool aligned16(const void *a, const void *b) { return ((uintptr_t)a % 16 == 0) && ((uintptr_t)b % 16 == 0); }
+
 int ensure_work(fftb_ffts_s *o)
 {
     if (o->work || o->work_bytes == 0) return FFTB_SUCCESS;
@@ -339,6 +342,7 @@ int fftb_ffts_create(int dtype, long long nx, long long ny, long long nz, long l
     else if (o->dim == 3) st = build_3d(o);
     else st = build_4d(o);
     if (st == FFTB_SUCCESS && o->dim == 3) st = fused3d_init(o->fused, dtype, nx, ny, nz);
+    if (st == FFTB_SUCCESS && o->dim == 4) st = fused4d_init(o->fused4, dtype, layout4d, nx, ny, nz, nw);
     if (st != FFTB_SUCCESS) {
         delete o;
         return st;
@@ -390,7 +394,13 @@ int fftb_ffts_forward(fftb_ffts o, const void *in, void *out)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
     if (!in || !out) return FFTB_ERROR_INVALID_VALUE;
-    if (o->fused.enabled) return fused3d_forward(o->fused, in, out, o->stream, o->timing ? &o->timer : nullptr);
+    LaunchTimer *tm = o->timing ? &o->timer : nullptr;
+    if (o->fused.enabled && aligned16(in, out)) return fused3d_forward(o->fused, in, out, o->stream, tm);
+    if (o->fused4.enabled && aligned16(in, out)) {
+        int st = ensure_work(o);
+        if (st != FFTB_SUCCESS) return st;
+        return fused4d_forward(o->fused4, in, out, o->work, o->stream, tm);
+    }
     return run(o, o->fwd, in, out, nullptr);
 }
 
@@ -398,7 +408,13 @@ int fftb_ffts_backward(fftb_ffts o, void *in, void *out)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
     if (!in || !out) return FFTB_ERROR_INVALID_VALUE;
-    if (o->fused.enabled) return fused3d_backward(o->fused, in, out, 1.0, o->stream, o->timing ? &o->timer : nullptr);
+    LaunchTimer *tm = o->timing ? &o->timer : nullptr;
+    if (o->fused.enabled && aligned16(in, out)) return fused3d_backward(o->fused, in, out, 1.0, o->stream, tm);
+    if (o->fused4.enabled && aligned16(in, out)) {
+        int st = ensure_work(o);
+        if (st != FFTB_SUCCESS) return st;
+        return fused4d_backward(o->fused4, in, out, o->work, 1.0, o->stream, tm);
+    }
     return run(o, o->bwd, in, out, nullptr);
 }
 
@@ -406,9 +422,15 @@ int fftb_ffts_backward_normalized(fftb_ffts o, void *in, void *out)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
     if (!in || !out) return FFTB_ERROR_INVALID_VALUE;
-    if (o->fused.enabled)
-        return fused3d_backward(o->fused, in, out, 1.0 / (double)(o->nx * o->ny * o->nz), o->stream,
-                                o->timing ? &o->timer : nullptr);
+    LaunchTimer *tm = o->timing ? &o->timer : nullptr;
+    if (o->fused.enabled && aligned16(in, out))
+        return fused3d_backward(o->fused, in, out, 1.0 / (double)(o->nx * o->ny * o->nz), o->stream, tm);
+    if (o->fused4.enabled && aligned16(in, out)) {
+        int st = ensure_work(o);
+        if (st != FFTB_SUCCESS) return st;
+        return fused4d_backward(o->fused4, in, out, o->work, 1.0 / (double)(o->nx * o->ny * o->nz * o->nw),
+                                o->stream, tm);
+    }
     return run(o, o->bwd_norm, in, out, nullptr);
 }
 
@@ -420,10 +442,12 @@ int fftb_ffts_poisson(fftb_ffts o, const void *rhs, void *sol, double sign)
     ep.scale = 1.0;
     ep.sign = sign;
     ep.mode = EP_SCALE | EP_POISSON;
-    if (o->fused.enabled) {
+    if ((o->fused.enabled || o->fused4.enabled) && aligned16(rhs, sol)) {
         int st = ensure_work(o);
         if (st != FFTB_SUCCESS) return st;
-        return fused3d_spectral(o->fused, rhs, sol, o->work, ep, o->stream, o->timing ? &o->timer : nullptr);
+        LaunchTimer *tm = o->timing ? &o->timer : nullptr;
+        if (o->fused.enabled) return fused3d_spectral(o->fused, rhs, sol, o->work, ep, o->stream, tm);
+        return fused4d_spectral(o->fused4, rhs, sol, o->work, ep, o->stream, tm);
     }
     return run(o, o->poisson, rhs, sol, &ep);
 }
@@ -437,10 +461,12 @@ int fftb_ffts_filter(fftb_ffts o, const void *in, void *out, double sigma, doubl
     ep.sign = poisson_sign;
     ep.gauss = 1.0 / (2.0 * sigma * sigma);
     ep.mode = EP_SCALE | EP_GAUSS | (poisson_sign != 0.0 ? EP_POISSON : 0);
-    if (o->fused.enabled) {
+    if ((o->fused.enabled || o->fused4.enabled) && aligned16(in, out)) {
         int st = ensure_work(o);
         if (st != FFTB_SUCCESS) return st;
-        return fused3d_spectral(o->fused, in, out, o->work, ep, o->stream, o->timing ? &o->timer : nullptr);
+        LaunchTimer *tm = o->timing ? &o->timer : nullptr;
+        if (o->fused.enabled) return fused3d_spectral(o->fused, in, out, o->work, ep, o->stream, tm);
+        return fused4d_spectral(o->fused4, in, out, o->work, ep, o->stream, tm);
     }
     return run(o, o->filter, in, out, &ep);
 }
@@ -529,6 +555,10 @@ int fftb_ffts_num_launches(fftb_ffts o, int which, int *launches)
     if (!o || !launches) return FFTB_ERROR_INVALID_HANDLE;
     if (o->fused.enabled) {
         *launches = fused3d_num_launches(o->fused, which);
+        return FFTB_SUCCESS;
+    }
+    if (o->fused4.enabled) {
+        *launches = fused4d_num_launches(o->fused4, which);
         return FFTB_SUCCESS;
     }
     const Program *p = which == 0 ? &o->fwd : which == 1 ? &o->bwd : which == 2 ? &o->poisson : &o->filter;

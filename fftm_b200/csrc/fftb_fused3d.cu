@@ -338,7 +338,9 @@ struct XColEp {
     int mode;  // EpMode bits (0: none)
     float scale_f, sign_f, gauss_f;
     double scale, sign, gauss;
+    // column -> wavenumbers: 3D col = ky*nzh + kz (kz half axis); 4D (nd4) col = (ky*nz + kz)*nwh + kw
     int nzh, ny, nz;
+    int nd4, nwh;
 };
 
 template <int NX> struct XColShape {
@@ -371,32 +373,63 @@ __device__ __forceinline__ void xcol_fft(cpx<R> (&v)[16], cpx<R> *scr, const cpx
     }
 }
 
-template <typename R, int NX, int MODE>  // MODE 0: forward, 1: inverse, 2: forward-multiply-inverse
+// MODE 0: forward, 1: inverse, 2: forward -> spectral multiply -> inverse (all in place),
+// 3: forward, written transposed: column col becomes the contiguous row tout[col][kx],
+// 4: inverse of 3: reads the rows tin[col][kx], writes the columns in place of `data`.
+// blockIdx.y selects a batch of column sets `bstride` elements apart (the transposed
+// side has NX * ncols elements per batch).
+template <typename R, int NX, int MODE>
 __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data, long long stride, int ncols,
+                                                   long long bstride, cpx<R> *__restrict__ tdata,
                                                    const cpx<R> *__restrict__ roots, XColEp ep)
 {
     using C = cpx<R>;
     constexpr int T = XColShape<NX>::T, W = XColShape<NX>::W;
+    constexpr int RP = NX + 1;  // row pitch of the transposing stage
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *scr = reinterpret_cast<C *>(smem_raw);
-    C *tw = scr + 16 * T * W;
+    C *tw = scr + (16 * T * W > W * RP ? 16 * T * W : W * RP);
     const int tid = threadIdx.x;
     const int t = tid / W, col = tid - (tid / W) * W;
     for (int i = tid; i < NX; i += 256) tw[i] = roots[i];
     const int cg0 = blockIdx.x * W + col;
     const bool ok = cg0 < ncols;
+    data += (size_t)blockIdx.y * bstride;
     C *p = data + (ok ? cg0 : 0);
     C v[16];
+    if (MODE == 4) {
+        // rows of the transposed input -> shared memory -> columns in registers
+        const C *src = tdata + (size_t)blockIdx.y * NX * ncols + (size_t)blockIdx.x * W * NX;
+        const int nrow = (ncols - (int)blockIdx.x * W) < W ? (ncols - (int)blockIdx.x * W) : W;
+        for (int e = tid; e < nrow * NX; e += 256) {
+            const int rr = e / NX, kx = e - (e / NX) * NX;
+            scr[rr * RP + kx] = src[(size_t)rr * NX + kx];
+        }
+        __syncthreads();
 #pragma unroll
-    for (int r = 0; r < 16; ++r) v[r] = p[(size_t)(t + T * r) * stride];
+        for (int r = 0; r < 16; ++r) v[r] = scr[col * RP + t + T * r];
+    } else {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) v[r] = p[(size_t)(t + T * r) * stride];
+    }
     __syncthreads();
-    if (MODE == 1) xcol_fft<R, NX, +1>(v, scr, tw, t, col);
+    if (MODE == 1 || MODE == 4) xcol_fft<R, NX, +1>(v, scr, tw, t, col);
     else xcol_fft<R, NX, -1>(v, scr, tw, t, col);
     if (MODE == 2) {
-        // wavenumbers: kx = t + T*j (output row), ky = col / nzh, kz = col % nzh (half axis)
-        const int ky_i = cg0 / ep.nzh, kz = cg0 - (cg0 / ep.nzh) * ep.nzh;
+        // wavenumbers: kx = t + T*j (output row); ky, kz, kw from the column
+        int ky_i, kz, kw = 0;
+        if (ep.nd4) {
+            const int cc = cg0 % (ep.nz * ep.nwh);
+            ky_i = cg0 / (ep.nz * ep.nwh);
+            const int kz_i = cc / ep.nwh;
+            kw = cc - kz_i * ep.nwh;
+            kz = kz_i <= ep.nz / 2 ? kz_i : kz_i - ep.nz;
+        } else {
+            ky_i = cg0 / ep.nzh;
+            kz = cg0 - (cg0 / ep.nzh) * ep.nzh;
+        }
         const int ky = ky_i <= ep.ny / 2 ? ky_i : ky_i - ep.ny;
-        const R kyz = R(ky * ky + kz * kz);
+        const R kyz = R(ky * ky + kz * kz + kw * kw);
         const R sc = sizeof(R) == 4 ? R(ep.scale_f) : R(ep.scale);
         const R sg = sizeof(R) == 4 ? R(ep.sign_f) : R(ep.sign);
         if ((ep.mode & (EP_POISSON | EP_GAUSS)) == EP_POISSON) {
@@ -425,7 +458,19 @@ __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data,
         }
         xcol_fft<R, NX, +1>(v, scr, tw, t, col);
     }
-    if (ok) {
+    if (MODE == 3) {
+        // columns in registers -> shared memory -> contiguous rows of the transposed output
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) scr[col * RP + t + T * j] = v[j];
+        __syncthreads();
+        C *dstp = tdata + (size_t)blockIdx.y * NX * ncols + (size_t)blockIdx.x * W * NX;
+        const int nrow = (ncols - (int)blockIdx.x * W) < W ? (ncols - (int)blockIdx.x * W) : W;
+        for (int e = tid; e < nrow * NX; e += 256) {
+            const int rr = e / NX, kx = e - (e / NX) * NX;
+            dstp[(size_t)rr * NX + kx] = scr[rr * RP + kx];
+        }
+    } else if (ok) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) p[(size_t)(t + T * j) * stride] = v[j];
     }
@@ -465,18 +510,20 @@ const PlaneEntry *find_plane(int dtype, int ny, int nz, int cl)
 
 struct XColEntry {
     int dtype, nx;
-    const void *fn[3];
+    const void *fn[5];
     size_t smem;
 };
 
 template <typename R, int NX> XColEntry xcol_entry(int dtype)
 {
     constexpr int T = XColShape<NX>::T, W = XColShape<NX>::W;
+    constexpr size_t scr = (size_t)16 * T * W > (size_t)W * (NX + 1) ? (size_t)16 * T * W : (size_t)W * (NX + 1);
     return XColEntry{dtype,
                      NX,
                      {(const void *)&xcol_kernel<R, NX, 0>, (const void *)&xcol_kernel<R, NX, 1>,
-                      (const void *)&xcol_kernel<R, NX, 2>},
-                     sizeof(cpx<R>) * ((size_t)16 * T * W + NX)};
+                      (const void *)&xcol_kernel<R, NX, 2>, (const void *)&xcol_kernel<R, NX, 3>,
+                      (const void *)&xcol_kernel<R, NX, 4>},
+                     sizeof(cpx<R>) * (scr + NX)};
 }
 
 const XColEntry *find_xcol(int dtype, int nx)
@@ -495,15 +542,14 @@ int configure(const void *fn, size_t smem)
     return FFTB_SUCCESS;
 }
 
-int launch_plane(const Fused3D &f, bool inverse, const void *in, void *out, double scale, cudaStream_t s,
-                 LaunchTimer *tm)
+// One launch of a plane kernel over `nplanes` planes.
+int launch_plane_n(const PlaneEntry *e, long long nplanes, bool inverse, const void *in, void *out, void *roots,
+                   double scale, cudaStream_t s, LaunchTimer *tm)
 {
-    const PlaneEntry *e = (const PlaneEntry *)f.plane;
-    void *roots = f.roots_plane;
     float sc = (float)scale;
     const void *fn = inverse ? e->inv : e->fwd;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(f.nx * e->cl));
+    cfg.gridDim = dim3((unsigned)(nplanes * e->cl));
     cfg.blockDim = dim3(e->nt);
     cfg.dynamicSmemBytes = inverse ? e->smem_inv : e->smem_fwd;
     cfg.stream = s;
@@ -517,11 +563,11 @@ int launch_plane(const Fused3D &f, bool inverse, const void *in, void *out, doub
         attr[0].val.clusterDim.z = 1;
         cfg.numAttrs = 1;
     }
-    const double bytes = (double)f.nx * f.ny * (4.0 * f.nz + 8.0 * (f.nz / 2 + 1));
+    const double bytes = (double)nplanes * e->ny * (4.0 * e->nz + 8.0 * (e->nz / 2 + 1));
     if (tm) {
         int st = timer_mark(tm, s,
                             std::string(inverse ? "plane_inv_kernel" : "plane_fwd_kernel") + "<f32," +
-                                std::to_string(f.ny) + "," + std::to_string(f.nz) + ",cl" + std::to_string(e->cl) +
+                                std::to_string(e->ny) + "," + std::to_string(e->nz) + ",cl" + std::to_string(e->cl) +
                                 ">",
                             bytes);
         if (st != FFTB_SUCCESS) return st;
@@ -543,12 +589,14 @@ int launch_plane(const Fused3D &f, bool inverse, const void *in, void *out, doub
     return set_status_from_cuda(err);
 }
 
-int launch_xcol(const Fused3D &f, int mode, void *data, const EpValues *ep, cudaStream_t s, LaunchTimer *tm)
+int launch_plane(const Fused3D &f, bool inverse, const void *in, void *out, double scale, cudaStream_t s,
+                 LaunchTimer *tm)
 {
-    const XColEntry *e = (const XColEntry *)f.xcol;
-    const long long nzh = f.nz / 2 + 1;
-    const long long ncols = f.ny * nzh;
-    const int W = 256 / (int)(f.nx / 16);
+    return launch_plane_n((const PlaneEntry *)f.plane, f.nx, inverse, in, out, f.roots_plane, scale, s, tm);
+}
+
+XColEp make_ep(const EpValues *ep)
+{
     XColEp x = {};
     x.mode = ep ? (ep->mode < 0 ? 0 : ep->mode) : 0;
     x.scale = ep ? ep->scale : 1.0;
@@ -557,22 +605,38 @@ int launch_xcol(const Fused3D &f, int mode, void *data, const EpValues *ep, cuda
     x.scale_f = (float)x.scale;
     x.sign_f = (float)x.sign;
     x.gauss_f = (float)x.gauss;
-    x.nzh = (int)nzh;
-    x.ny = (int)f.ny;
-    x.nz = (int)f.nz;
+    return x;
+}
+
+// One launch of a column kernel: ncols columns `stride` apart per batch, nbatch batches.
+int launch_xcol_n(const XColEntry *e, int mode, void *data, long long stride, long long ncols, long long nbatch,
+                  long long bstride, void *tdata, void *roots, XColEp x, cudaStream_t s, LaunchTimer *tm)
+{
+    const int W = 256 / (e->nx / 16);
     if (tm) {
-        static const char *mn[] = {"fwd", "inv", "sandwich"};
-        int st = timer_mark(tm, s, std::string("xcol_kernel<f32,") + std::to_string(f.nx) + "," + mn[mode] + ">",
-                            (double)f.nx * ncols * 16.0);
+        static const char *mn[] = {"fwd", "inv", "sandwich", "fwd_t", "inv_t"};
+        int st = timer_mark(tm, s, std::string("xcol_kernel<f32,") + std::to_string(e->nx) + "," + mn[mode] + ">",
+                            (double)e->nx * ncols * nbatch * 16.0);
         if (st != FFTB_SUCCESS) return st;
     }
     float2 *d = (float2 *)data;
-    long long stride = ncols;
+    float2 *td = (float2 *)tdata;
     int nc = (int)ncols;
-    const float2 *rt = (const float2 *)f.roots_x;
-    void *args[] = {&d, &stride, &nc, &rt, &x};
-    const unsigned grid = (unsigned)((ncols + W - 1) / W);
-    return set_status_from_cuda(cudaLaunchKernel(e->fn[mode], dim3(grid), dim3(256), args, e->smem, s));
+    const float2 *rt = (const float2 *)roots;
+    void *args[] = {&d, &stride, &nc, &bstride, &td, &rt, &x};
+    const dim3 grid((unsigned)((ncols + W - 1) / W), (unsigned)nbatch);
+    return set_status_from_cuda(cudaLaunchKernel(e->fn[mode], grid, dim3(256), args, e->smem, s));
+}
+
+int launch_xcol(const Fused3D &f, int mode, void *data, const EpValues *ep, cudaStream_t s, LaunchTimer *tm)
+{
+    const long long nzh = f.nz / 2 + 1;
+    const long long ncols = f.ny * nzh;
+    XColEp x = make_ep(ep);
+    x.nzh = (int)nzh;
+    x.ny = (int)f.ny;
+    x.nz = (int)f.nz;
+    return launch_xcol_n((const XColEntry *)f.xcol, mode, data, ncols, ncols, 1, 0, nullptr, f.roots_x, x, s, tm);
 }
 
 } // namespace
@@ -606,7 +670,7 @@ int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz
     int st;
     if ((st = configure(pe->fwd, pe->smem_fwd)) != FFTB_SUCCESS) return st;
     if ((st = configure(pe->inv, pe->smem_inv)) != FFTB_SUCCESS) return st;
-    for (int m = 0; m < 3; ++m)
+    for (int m = 0; m < 5; ++m)
         if ((st = configure(xe->fn[m], xe->smem)) != FFTB_SUCCESS) return st;
     const int nmax = (int)(ny > nz ? ny : nz);
     if ((st = engine_roots(dtype, nmax, &f.roots_plane)) != FFTB_SUCCESS) return st;
@@ -649,6 +713,113 @@ int fused3d_num_launches(const Fused3D &f, int which)
 {
     (void)f;
     return which <= 1 ? 2 : 3;
+}
+
+// ------------------------------------------------------------------ 4D slab / native_xzwy
+// real [x][y][z][w]; work / slab spectrum [x][y][kz][kw<nw/2+1]; native spectrum
+// [ky][kz][kw][kx].  Stages: the (z,w) plane R2C over the nx*ny planes (the 3D plane
+// kernels), the y FFT (column kernel batched over x), the x FFT (column kernel; for
+// native_xzwy written transposed so kx becomes the contiguous axis).
+int fused4d_init(Fused4D &f, int dtype, int layout, long long nx, long long ny, long long nz, long long nw)
+{
+    f.enabled = false;
+    f.dtype = dtype;
+    f.layout = layout;
+    f.nx = nx; f.ny = ny; f.nz = nz; f.nw = nw;
+    if (dtype != FFTB_F32 || (layout != FFTB_4D_SLAB && layout != FFTB_4D_NATIVE_XZWY)) return FFTB_SUCCESS;
+    if (getenv("FFTB_DISABLE_FUSED3D")) return FFTB_SUCCESS;
+    const PlaneEntry *pe = find_plane(dtype, (int)nz, (int)nw, 1);
+    const XColEntry *xe = find_xcol(dtype, (int)nx);
+    const XColEntry *ye = find_xcol(dtype, (int)ny);
+    if (!pe || !xe || !ye || pe->smem_fwd > 113 * 1024 || pe->smem_inv > 113 * 1024) return FFTB_SUCCESS;
+    int st;
+    if ((st = configure(pe->fwd, pe->smem_fwd)) != FFTB_SUCCESS) return st;
+    if ((st = configure(pe->inv, pe->smem_inv)) != FFTB_SUCCESS) return st;
+    for (const XColEntry *e : {xe, ye})
+        for (int m = 0; m < 5; ++m)
+            if ((st = configure(e->fn[m], e->smem)) != FFTB_SUCCESS) return st;
+    const int nmax = (int)(nz > nw ? nz : nw);
+    if ((st = engine_roots(dtype, nmax, &f.roots_plane)) != FFTB_SUCCESS) return st;
+    if ((st = engine_roots(dtype, (int)nx, &f.roots_x)) != FFTB_SUCCESS) return st;
+    if ((st = engine_roots(dtype, (int)ny, &f.roots_y)) != FFTB_SUCCESS) return st;
+    f.plane = pe;
+    f.xcol = xe;
+    f.ycol = ye;
+    f.enabled = true;
+    return FFTB_SUCCESS;
+}
+
+namespace {
+XColEp ep4(const Fused4D &f, const EpValues *ep)
+{
+    XColEp x = make_ep(ep);
+    x.nd4 = 1;
+    x.ny = (int)f.ny;
+    x.nz = (int)f.nz;
+    x.nwh = (int)(f.nw / 2 + 1);
+    x.nzh = 1;
+    return x;
+}
+} // namespace
+
+// out: the spectrum in the object's layout; work: slab-layout scratch (native only)
+int fused4d_forward(const Fused4D &f, const void *in, void *out, void *work, cudaStream_t s, LaunchTimer *t)
+{
+    const long long C = f.nz * (f.nw / 2 + 1), YC = f.ny * C;
+    const bool native = f.layout == FFTB_4D_NATIVE_XZWY;
+    void *slab = native ? work : out;
+    if (native && !work) return FFTB_ERROR_NO_WORK_AREA;
+    const PlaneEntry *pe = (const PlaneEntry *)f.plane;
+    int st = launch_plane_n(pe, f.nx * f.ny, false, in, slab, f.roots_plane, 1.0, s, t);
+    if (st == FFTB_SUCCESS)
+        st = launch_xcol_n((const XColEntry *)f.ycol, 0, slab, C, C, f.nx, YC, nullptr, f.roots_y, ep4(f, nullptr), s, t);
+    if (st == FFTB_SUCCESS)
+        st = launch_xcol_n((const XColEntry *)f.xcol, native ? 3 : 0, slab, YC, YC, 1, 0, out, f.roots_x,
+                           ep4(f, nullptr), s, t);
+    if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
+    return st;
+}
+
+int fused4d_backward(const Fused4D &f, void *in, void *out, void *work, double scale, cudaStream_t s, LaunchTimer *t)
+{
+    const long long C = f.nz * (f.nw / 2 + 1), YC = f.ny * C;
+    const bool native = f.layout == FFTB_4D_NATIVE_XZWY;
+    void *slab = native ? work : in;
+    if (native && !work) return FFTB_ERROR_NO_WORK_AREA;
+    const PlaneEntry *pe = (const PlaneEntry *)f.plane;
+    int st = launch_xcol_n((const XColEntry *)f.xcol, native ? 4 : 1, slab, YC, YC, 1, 0, in, f.roots_x,
+                           ep4(f, nullptr), s, t);
+    if (st == FFTB_SUCCESS)
+        st = launch_xcol_n((const XColEntry *)f.ycol, 1, slab, C, C, f.nx, YC, nullptr, f.roots_y, ep4(f, nullptr), s, t);
+    if (st == FFTB_SUCCESS) st = launch_plane_n(pe, f.nx * f.ny, true, slab, out, f.roots_plane, scale, s, t);
+    if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
+    return st;
+}
+
+int fused4d_spectral(const Fused4D &f, const void *in, void *out, void *work, const EpValues &ep, cudaStream_t s,
+                     LaunchTimer *t)
+{
+    if (!work) return FFTB_ERROR_NO_WORK_AREA;
+    const long long C = f.nz * (f.nw / 2 + 1), YC = f.ny * C;
+    const PlaneEntry *pe = (const PlaneEntry *)f.plane;
+    int st = launch_plane_n(pe, f.nx * f.ny, false, in, work, f.roots_plane, 1.0, s, t);
+    if (st == FFTB_SUCCESS)
+        st = launch_xcol_n((const XColEntry *)f.ycol, 0, work, C, C, f.nx, YC, nullptr, f.roots_y, ep4(f, nullptr), s, t);
+    if (st == FFTB_SUCCESS)
+        st = launch_xcol_n((const XColEntry *)f.xcol, 2, work, YC, YC, 1, 0, nullptr, f.roots_x, ep4(f, &ep), s, t);
+    if (st == FFTB_SUCCESS)
+        st = launch_xcol_n((const XColEntry *)f.ycol, 1, work, C, C, f.nx, YC, nullptr, f.roots_y, ep4(f, nullptr), s, t);
+    if (st == FFTB_SUCCESS)
+        st = launch_plane_n(pe, f.nx * f.ny, true, work, out, f.roots_plane,
+                            1.0 / (double)(f.nx * f.ny * f.nz * f.nw), s, t);
+    if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
+    return st;
+}
+
+int fused4d_num_launches(const Fused4D &f, int which)
+{
+    (void)f;
+    return which <= 1 ? 3 : 5;
 }
 
 } // namespace fftb

@@ -26,4 +26,20 @@ int fused3d_spectral(const Fused3D &f, const void *in, void *out, void *work, co
                      LaunchTimer *t);
 int fused3d_num_launches(const Fused3D &f, int which);
 
+// 4D slab / native_xzwy with power-of-two (z, w) planes and x, y column kernels.
+struct Fused4D {
+    bool enabled = false;
+    int dtype = 0, layout = 0;
+    long long nx = 0, ny = 0, nz = 0, nw = 0;
+    const void *plane = nullptr, *xcol = nullptr, *ycol = nullptr;
+    void *roots_plane = nullptr, *roots_x = nullptr, *roots_y = nullptr;
+};
+int fused4d_init(Fused4D &f, int dtype, int layout, long long nx, long long ny, long long nz, long long nw);
+int fused4d_forward(const Fused4D &f, const void *in, void *out, void *work, cudaStream_t s, LaunchTimer *t);
+int fused4d_backward(const Fused4D &f, void *in, void *out, void *work, double scale, cudaStream_t s,
+                     LaunchTimer *t);
+int fused4d_spectral(const Fused4D &f, const void *in, void *out, void *work, const EpValues &ep, cudaStream_t s,
+                     LaunchTimer *t);
+int fused4d_num_launches(const Fused4D &f, int which);
+
 } // namespace fftb
