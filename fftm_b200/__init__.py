@@ -308,6 +308,21 @@ class ffts:
         fn = _lib.load().fftb_ffts_backward_normalized if normalized else _lib.load().fftb_ffts_backward
         _check(fn(self._h, _ptr(complex_in), _ptr(real_out)), "ffts::backward")
 
+    def forward_adjoint(self, grad_spectrum, grad_real, stream=None):
+        """Transpose of forward(): grad_real = C2R(W * grad_spectrum), W = 1/2 on interior
+        half-axis bins.  grad_spectrum may be overwritten."""
+        self._ensure()
+        self._bind(stream)
+        _check(_lib.load().fftb_ffts_forward_adjoint(self._h, _ptr(grad_spectrum), _ptr(grad_real)),
+               "ffts::forward_adjoint")
+
+    def backward_adjoint(self, grad_real, grad_spectrum, stream=None):
+        """Transpose of the unnormalised backward(): grad_spectrum = W2 * R2C(grad_real)."""
+        self._ensure()
+        self._bind(stream)
+        _check(_lib.load().fftb_ffts_backward_adjoint(self._h, _ptr(grad_real), _ptr(grad_spectrum)),
+               "ffts::backward_adjoint")
+
     def poisson(self, rhs, solution, sign=-1.0, stream=None):
         """u = C2R(sign * R2C(f) / |k|^2) / N, k=0 -> 0, fused into the FFT passes."""
         self._ensure()

@@ -20,7 +20,7 @@ EXPORTS = [
     "fftb_ffts_set_work_area", "fftb_ffts_set_stream", "fftb_ffts_forward", "fftb_ffts_backward",
     "fftb_ffts_backward_normalized", "fftb_ffts_poisson", "fftb_ffts_filter", "fftb_ffts_spectrum_poisson",
     "fftb_ffts_num_launches", "fftb_ffts_timing_enable", "fftb_ffts_timing_read",
-    "fftb_poisson3d_f32_noalloc",
+    "fftb_poisson3d_f32_noalloc", "fftb_ffts_forward_adjoint", "fftb_ffts_backward_adjoint",
 ]
 
 _lib = None
@@ -69,6 +69,8 @@ def load():
     L.fftb_ffts_timing_enable.argtypes = [c_vp, c_int]
     L.fftb_ffts_timing_read.argtypes = [c_vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(c_d),
                                         ctypes.c_char_p, c_int, c_int, ip]
+    L.fftb_ffts_forward_adjoint.argtypes = [c_vp, c_vp, c_vp]
+    L.fftb_ffts_backward_adjoint.argtypes = [c_vp, c_vp, c_vp]
     L.fftb_poisson3d_f32_noalloc.argtypes = [c_vp, c_vp, c_ll, c_ll, c_ll, c_d, c_vp]
     for name in EXPORTS:
         if name not in ("fftb_status_string", "fftb_version", "fftb_last_error_message"):

@@ -201,6 +201,7 @@ int program_add(Program &prog, int dtype, const AxisPass &p)
     a.ep_scale = p.ep_scale;
     a.ep_sign = p.ep_sign;
     a.ep_gauss = p.ep_gauss;
+    a.ep_hw = p.ep_hw;
     a.ep_naxes = (int)p.ep_axes.size();
     if (a.ep_naxes > 4) return FFTB_ERROR_INVALID_VALUE;
     for (int i = 0; i < a.ep_naxes; ++i) {

@@ -42,7 +42,7 @@ struct AxisPass {
     int in_buf = B_IN, out_buf = B_OUT;
     long long in_base = 0, out_base = 0;  // element offsets inside the buffers
     int ep_mode = 0;
-    double ep_scale = 1.0, ep_sign = -1.0, ep_gauss = 0.0;
+    double ep_scale = 1.0, ep_sign = -1.0, ep_gauss = 0.0, ep_hw = 1.0;
     std::vector<EpAxis> ep_axes;
     int ep_dynamic = 0;         // epilogue parameters supplied at execution
 };
@@ -70,7 +70,7 @@ struct Program {
 
 // Dynamic epilogue values for one execution.
 struct EpValues {
-    double scale = 1.0, sign = -1.0, gauss = 0.0;
+    double scale = 1.0, sign = -1.0, gauss = 0.0, hw = 1.0;
     int mode = -1;  // -1: keep the built mode
 };
 

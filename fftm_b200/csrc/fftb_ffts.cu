@@ -22,6 +22,7 @@ struct fftb_ffts_s {
     int dtype = 0, dim = 0, layout = 0;
     long long nx = 0, ny = 0, nz = 0, nw = 0;
     Program fwd, bwd, bwd_norm, poisson, filter;
+    Program fwd_adj, bwd_adj;  // adjoints of forward (weighted C2R) and of backward (weighted R2C)
     size_t work_bytes = 0;
     void *work = nullptr;
     bool own_work = false;
@@ -63,6 +64,15 @@ AxisPass sandwich(AxisPass p, std::vector<EpAxis> axes)
     return p;
 }
 
+// EP_HALFW epilogue: interior bins of the half axis (batch dim `dim_id`, full length n) times w
+AxisPass halfw(AxisPass p, int dim_id, long long n, double w)
+{
+    p.ep_mode |= EP_HALFW;
+    p.ep_hw = w;
+    p.ep_axes = {EpAxis{0, dim_id, (int)n, 1}};
+    return p;
+}
+
 #define TRY(x)                                                                                                        \
     do {                                                                                                              \
         int _s = (x);                                                                                                 \
@@ -84,6 +94,10 @@ int build_2d(fftb_ffts_s *o)
     TRY(program_add(o->bwd, d, c2r));
     TRY(program_add(o->bwd_norm, d, xi));
     TRY(program_add(o->bwd_norm, d, with_scale(c2r, invN)));
+    TRY(program_add(o->fwd_adj, d, halfw(xi, 1, ny, 0.5)));
+    TRY(program_add(o->fwd_adj, d, c2r));
+    TRY(program_add(o->bwd_adj, d, r2c));
+    TRY(program_add(o->bwd_adj, d, halfw(xf, 1, ny, 2.0)));
     for (int f = 0; f < 2; ++f) {
         Program &pr = f ? o->filter : o->poisson;
         AxisPass a = r2c;
@@ -123,6 +137,12 @@ int build_3d(fftb_ffts_s *o)
     TRY(program_add(o->bwd_norm, d, xi));
     TRY(program_add(o->bwd_norm, d, yi));
     TRY(program_add(o->bwd_norm, d, with_scale(zc, invN)));
+    TRY(program_add(o->fwd_adj, d, halfw(xi, 2, nz, 0.5)));
+    TRY(program_add(o->fwd_adj, d, yi));
+    TRY(program_add(o->fwd_adj, d, zc));
+    TRY(program_add(o->bwd_adj, d, zr));
+    TRY(program_add(o->bwd_adj, d, yf));
+    TRY(program_add(o->bwd_adj, d, halfw(xf, 2, nz, 2.0)));
     for (int f = 0; f < 2; ++f) {
         Program &pr = f ? o->filter : o->poisson;
         AxisPass a = zr;
@@ -174,6 +194,14 @@ int build_4d(fftb_ffts_s *o)
             TRY(program_add(o->fwd, d, zf));
             TRY(program_add(o->fwd, d, yf));
             TRY(program_add(o->fwd, d, xf));
+            TRY(program_add(o->fwd_adj, d, halfw(on(inv(xf), B_IN, B_IN), 3, nw, 0.5)));
+            TRY(program_add(o->fwd_adj, d, on(inv(yf), B_IN, B_IN)));
+            TRY(program_add(o->fwd_adj, d, on(inv(zf), B_IN, B_IN)));
+            TRY(program_add(o->fwd_adj, d, wc));
+            TRY(program_add(o->bwd_adj, d, wr));
+            TRY(program_add(o->bwd_adj, d, zf));
+            TRY(program_add(o->bwd_adj, d, yf));
+            TRY(program_add(o->bwd_adj, d, halfw(xf, 3, nw, 2.0)));
             for (int nrm = 0; nrm < 2; ++nrm) {
                 Program &pr = nrm ? o->bwd_norm : o->bwd;
                 TRY(program_add(pr, d, on(inv(xf), B_IN, B_IN)));
@@ -192,6 +220,14 @@ int build_4d(fftb_ffts_s *o)
             TRY(program_add(o->fwd, d, xp));
             AxisPass xq = mkpass(K_C2C_INV, nx, 1, ny * C,
                                  {Dim{nwh, nx, 1, 3}, Dim{nz, nwh * nx, nwh, 2}, Dim{ny, C * nx, C, 1}}, B_IN, B_WORK);
+            TRY(program_add(o->fwd_adj, d, halfw(xq, 3, nw, 0.5)));
+            TRY(program_add(o->fwd_adj, d, on(inv(yf), B_WORK, B_WORK)));
+            TRY(program_add(o->fwd_adj, d, on(inv(zf), B_WORK, B_WORK)));
+            TRY(program_add(o->fwd_adj, d, on(wc, B_WORK, B_OUT)));
+            TRY(program_add(o->bwd_adj, d, on(wr, B_IN, B_WORK)));
+            TRY(program_add(o->bwd_adj, d, on(zf, B_WORK, B_WORK)));
+            TRY(program_add(o->bwd_adj, d, on(yf, B_WORK, B_WORK)));
+            TRY(program_add(o->bwd_adj, d, halfw(xp, 3, nw, 2.0)));
             for (int nrm = 0; nrm < 2; ++nrm) {
                 Program &pr = nrm ? o->bwd_norm : o->bwd;
                 TRY(program_add(pr, d, xq));
@@ -234,6 +270,14 @@ int build_4d(fftb_ffts_s *o)
         TRY(program_add(o->fwd, d, zf));
         TRY(program_add(o->fwd, d, yf));
         TRY(program_add(o->fwd, d, xp));
+        TRY(program_add(o->fwd_adj, d, halfw(xq, 3, nw, 0.5)));
+        TRY(program_add(o->fwd_adj, d, inv(yf)));
+        TRY(program_add(o->fwd_adj, d, inv(zf)));
+        TRY(program_add(o->fwd_adj, d, wc));
+        TRY(program_add(o->bwd_adj, d, wr));
+        TRY(program_add(o->bwd_adj, d, zf));
+        TRY(program_add(o->bwd_adj, d, yf));
+        TRY(program_add(o->bwd_adj, d, halfw(xp, 3, nw, 2.0)));
         for (int nrm = 0; nrm < 2; ++nrm) {
             Program &pr = nrm ? o->bwd_norm : o->bwd;
             TRY(program_add(pr, d, xq));
@@ -469,6 +513,36 @@ int fftb_ffts_filter(fftb_ffts o, const void *in, void *out, double sigma, doubl
         return fused4d_spectral(o->fused4, in, out, o->work, ep, o->stream, tm);
     }
     return run(o, o->filter, in, out, &ep);
+}
+
+int fftb_ffts_forward_adjoint(fftb_ffts o, void *grad_spectrum, void *grad_real)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (!grad_spectrum || !grad_real) return FFTB_ERROR_INVALID_VALUE;
+    LaunchTimer *tm = o->timing ? &o->timer : nullptr;
+    if (o->fused.enabled && aligned16(grad_spectrum, grad_real))
+        return fused3d_forward_adjoint(o->fused, grad_spectrum, grad_real, o->stream, tm);
+    if (o->fused4.enabled && aligned16(grad_spectrum, grad_real)) {
+        int st = ensure_work(o);
+        if (st != FFTB_SUCCESS) return st;
+        return fused4d_forward_adjoint(o->fused4, grad_spectrum, grad_real, o->work, o->stream, tm);
+    }
+    return run(o, o->fwd_adj, grad_spectrum, grad_real, nullptr);
+}
+
+int fftb_ffts_backward_adjoint(fftb_ffts o, const void *grad_real, void *grad_spectrum)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (!grad_spectrum || !grad_real) return FFTB_ERROR_INVALID_VALUE;
+    LaunchTimer *tm = o->timing ? &o->timer : nullptr;
+    if (o->fused.enabled && aligned16(grad_spectrum, grad_real))
+        return fused3d_backward_adjoint(o->fused, grad_real, grad_spectrum, o->stream, tm);
+    if (o->fused4.enabled && aligned16(grad_spectrum, grad_real)) {
+        int st = ensure_work(o);
+        if (st != FFTB_SUCCESS) return st;
+        return fused4d_backward_adjoint(o->fused4, grad_real, grad_spectrum, o->work, o->stream, tm);
+    }
+    return run(o, o->bwd_adj, grad_real, grad_spectrum, nullptr);
 }
 
 int fftb_ffts_spectrum_poisson(fftb_ffts o, void *spec, double sign, double scale)

@@ -12,11 +12,11 @@
 //              scale (1/N for the normalised inverse and the Poisson solve).
 //
 // All FFTs are register resident (fftb_regfft.cuh); shared memory holds the
-// plane between the z and y stages.  A 256x256 plane (133 KB of spectrum) is
-// split over a 2-CTA cluster: each CTA transforms half of the rows along z, and
-// the y FFT's first radix-2 step is taken across the pair through distributed
-// shared memory (CTA 0 forms x[m] + x[m+M] and yields the even ky, CTA 1 forms
-// (x[m] - x[m+M]) w^m and yields the odd ky), so no plane ever round-trips
+// plane between the z and y stages.  A plane too large for one CTA (a 256x256
+// plane is 133 KB of spectrum) is split over a cluster of 2 or 4 CTAs: each CTA
+// transforms a block of rows along z and owns a block of kz columns for the y
+// stage, and the data that changes owner in between is pushed into the owner's
+// shared memory with distributed-shared-memory stores, so no plane round-trips
 // through global memory between the z and y stages.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
@@ -39,8 +39,9 @@ namespace fftb {
 // Slot s < NZ/2 is spectrum column kz = s, except slot 0, which packs the two
 // real-per-row columns kz = 0 and kz = NZ/2 as one complex column (kz=0 in the
 // real part, kz=NZ/2 in the imaginary part); their y FFTs are separated by
-// Hermitian symmetry (forward) or simply stay packed (inverse, where the C2R
-// keeps only the real parts of kz = 0 and NZ/2).  Data that changes owner
+// Hermitian symmetry (forward), or the two columns are made Hermitian in ky before
+// one packed inverse FFT (inverse, where the C2R keeps only the real parts of the
+// kz = 0 and NZ/2 results).  Data that changes owner
 // between the stages is pushed with distributed-shared-memory stores, so no CTA
 // ever reads another CTA's shared memory.
 template <int NY, int NZ, int CL> struct PlaneShape {
@@ -259,11 +260,19 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT)
 #pragma unroll
             for (int r = 0; r < 16; ++r) v[r] = col[t + TY * r];
             if (ok && c == 0 && sl == 0) {
-                // packed slot: W = X0 + i XN
+                // packed slot: W = H0 + i HN with H(ky) = (X(ky) + conj X(-ky)) / 2 for the columns
+                // kz = 0 (X0, staged in col) and kz = NZ/2 (XN, read here).  The inverse y FFT of
+                // H is the real part of that of X, which is all the C2R keeps of these two
+                // columns; so the pair packs exactly, Hermitian-consistent input or not.
 #pragma unroll
                 for (int r = 0; r < 16; ++r) {
-                    const C xn = iplane[(size_t)(t + TY * r) * (NZ / 2 + 1) + NZ / 2];
-                    v[r] = mk<R>(v[r].x - xn.y, v[r].y + xn.x);
+                    const int ky = t + TY * r, km = (NY - ky) & (NY - 1);
+                    const C x0m = col[km];
+                    const C xnk = iplane[(size_t)ky * (NZ / 2 + 1) + NZ / 2];
+                    const C xnm = iplane[(size_t)km * (NZ / 2 + 1) + NZ / 2];
+                    const C h0 = cscale(cadd(v[r], cconj(x0m)), R(0.5));
+                    const C hn = cscale(cadd(xnk, cconj(xnm)), R(0.5));
+                    v[r] = mk<R>(h0.x - hn.y, h0.y + hn.x);
                 }
             }
             regfft_warp<R, NY, +1>(v, col, twy, t);
@@ -341,6 +350,10 @@ struct XColEp {
     // column -> wavenumbers: 3D col = ky*nzh + kz (kz half axis); 4D (nd4) col = (ky*nz + kz)*nwh + kw
     int nzh, ny, nz;
     int nd4, nwh;
+    // EP_HALFW: interior bins of the half axis (column index mod (hn/2+1)) times hw
+    int hn;
+    float hw_f;
+    double hw;
 };
 
 template <int NX> struct XColShape {
@@ -457,6 +470,14 @@ __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data,
             }
         }
         xcol_fft<R, NX, +1>(v, scr, tw, t, col);
+    }
+    if (MODE != 2 && (ep.mode & EP_HALFW)) {
+        const int ih = cg0 % (ep.hn / 2 + 1);
+        if (ih != 0 && 2 * ih != ep.hn) {
+            const R w = sizeof(R) == 4 ? R(ep.hw_f) : R(ep.hw);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = cscale(v[j], w);
+        }
     }
     if (MODE == 3) {
         // columns in registers -> shared memory -> contiguous rows of the transposed output
@@ -605,6 +626,8 @@ XColEp make_ep(const EpValues *ep)
     x.scale_f = (float)x.scale;
     x.sign_f = (float)x.sign;
     x.gauss_f = (float)x.gauss;
+    x.hw = ep ? ep->hw : 1.0;
+    x.hw_f = (float)x.hw;
     return x;
 }
 
@@ -636,6 +659,7 @@ int launch_xcol(const Fused3D &f, int mode, void *data, const EpValues *ep, cuda
     x.nzh = (int)nzh;
     x.ny = (int)f.ny;
     x.nz = (int)f.nz;
+    x.hn = (int)f.nz;
     return launch_xcol_n((const XColEntry *)f.xcol, mode, data, ncols, ncols, 1, 0, nullptr, f.roots_x, x, s, tm);
 }
 
@@ -709,6 +733,30 @@ int fused3d_spectral(const Fused3D &f, const void *in, void *out, void *work, co
     return st;
 }
 
+// adjoint of the forward R2C: C2R of the gradient with interior kz bins weighted 1/2
+int fused3d_forward_adjoint(const Fused3D &f, void *gspec, void *greal, cudaStream_t s, LaunchTimer *t)
+{
+    EpValues ep;
+    ep.mode = EP_HALFW;
+    ep.hw = 0.5;
+    int st = launch_xcol(f, 1, gspec, &ep, s, t);
+    if (st == FFTB_SUCCESS) st = launch_plane(f, true, gspec, greal, 1.0, s, t);
+    if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
+    return st;
+}
+
+// adjoint of the (unnormalised) C2R: R2C of the gradient with interior kz bins doubled
+int fused3d_backward_adjoint(const Fused3D &f, const void *greal, void *gspec, cudaStream_t s, LaunchTimer *t)
+{
+    EpValues ep;
+    ep.mode = EP_HALFW;
+    ep.hw = 2.0;
+    int st = launch_plane(f, false, greal, gspec, 1.0, s, t);
+    if (st == FFTB_SUCCESS) st = launch_xcol(f, 0, gspec, &ep, s, t);
+    if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
+    return st;
+}
+
 int fused3d_num_launches(const Fused3D &f, int which)
 {
     (void)f;
@@ -758,6 +806,7 @@ XColEp ep4(const Fused4D &f, const EpValues *ep)
     x.nz = (int)f.nz;
     x.nwh = (int)(f.nw / 2 + 1);
     x.nzh = 1;
+    x.hn = (int)f.nw;
     return x;
 }
 } // namespace
@@ -812,6 +861,45 @@ int fused4d_spectral(const Fused4D &f, const void *in, void *out, void *work, co
     if (st == FFTB_SUCCESS)
         st = launch_plane_n(pe, f.nx * f.ny, true, work, out, f.roots_plane,
                             1.0 / (double)(f.nx * f.ny * f.nz * f.nw), s, t);
+    if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
+    return st;
+}
+
+int fused4d_forward_adjoint(const Fused4D &f, void *gspec, void *greal, void *work, cudaStream_t s, LaunchTimer *t)
+{
+    const long long C = f.nz * (f.nw / 2 + 1), YC = f.ny * C;
+    const bool native = f.layout == FFTB_4D_NATIVE_XZWY;
+    void *slab = native ? work : gspec;
+    if (native && !work) return FFTB_ERROR_NO_WORK_AREA;
+    EpValues ev;
+    ev.mode = EP_HALFW;
+    ev.hw = 0.5;
+    int st = launch_xcol_n((const XColEntry *)f.xcol, native ? 4 : 1, slab, YC, YC, 1, 0, gspec, f.roots_x,
+                           ep4(f, &ev), s, t);
+    if (st == FFTB_SUCCESS)
+        st = launch_xcol_n((const XColEntry *)f.ycol, 1, slab, C, C, f.nx, YC, nullptr, f.roots_y, ep4(f, nullptr), s, t);
+    if (st == FFTB_SUCCESS)
+        st = launch_plane_n((const PlaneEntry *)f.plane, f.nx * f.ny, true, slab, greal, f.roots_plane, 1.0, s, t);
+    if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
+    return st;
+}
+
+int fused4d_backward_adjoint(const Fused4D &f, const void *greal, void *gspec, void *work, cudaStream_t s,
+                             LaunchTimer *t)
+{
+    const long long C = f.nz * (f.nw / 2 + 1), YC = f.ny * C;
+    const bool native = f.layout == FFTB_4D_NATIVE_XZWY;
+    void *slab = native ? work : gspec;
+    if (native && !work) return FFTB_ERROR_NO_WORK_AREA;
+    EpValues ev;
+    ev.mode = EP_HALFW;
+    ev.hw = 2.0;
+    int st = launch_plane_n((const PlaneEntry *)f.plane, f.nx * f.ny, false, greal, slab, f.roots_plane, 1.0, s, t);
+    if (st == FFTB_SUCCESS)
+        st = launch_xcol_n((const XColEntry *)f.ycol, 0, slab, C, C, f.nx, YC, nullptr, f.roots_y, ep4(f, nullptr), s, t);
+    if (st == FFTB_SUCCESS)
+        st = launch_xcol_n((const XColEntry *)f.xcol, native ? 3 : 0, slab, YC, YC, 1, 0, gspec, f.roots_x,
+                           ep4(f, &ev), s, t);
     if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
     return st;
 }

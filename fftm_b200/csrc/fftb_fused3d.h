@@ -24,6 +24,8 @@ int fused3d_forward(const Fused3D &f, const void *in, void *out, cudaStream_t s,
 int fused3d_backward(const Fused3D &f, void *in, void *out, double scale, cudaStream_t s, LaunchTimer *t);
 int fused3d_spectral(const Fused3D &f, const void *in, void *out, void *work, const EpValues &ep, cudaStream_t s,
                      LaunchTimer *t);
+int fused3d_forward_adjoint(const Fused3D &f, void *gspec, void *greal, cudaStream_t s, LaunchTimer *t);
+int fused3d_backward_adjoint(const Fused3D &f, const void *greal, void *gspec, cudaStream_t s, LaunchTimer *t);
 int fused3d_num_launches(const Fused3D &f, int which);
 
 // 4D slab / native_xzwy with power-of-two (z, w) planes and x, y column kernels.
@@ -40,6 +42,9 @@ int fused4d_backward(const Fused4D &f, void *in, void *out, void *work, double s
                      LaunchTimer *t);
 int fused4d_spectral(const Fused4D &f, const void *in, void *out, void *work, const EpValues &ep, cudaStream_t s,
                      LaunchTimer *t);
+int fused4d_forward_adjoint(const Fused4D &f, void *gspec, void *greal, void *work, cudaStream_t s, LaunchTimer *t);
+int fused4d_backward_adjoint(const Fused4D &f, const void *greal, void *gspec, void *work, cudaStream_t s,
+                             LaunchTimer *t);
 int fused4d_num_launches(const Fused4D &f, int which);
 
 } // namespace fftb

@@ -21,6 +21,7 @@ enum EpMode : int {
     EP_SCALE = 1,    // multiply by ep_scale
     EP_POISSON = 2,  // multiply by ep_sign / |k|^2 (0 at k = 0)
     EP_GAUSS = 4,    // multiply by exp(-|k|^2 * ep_gauss)
+    EP_HALFW = 8,    // multiply interior bins of the half (R2C) axis by ep_hw (adjoint weights)
 };
 
 // Everything one pass launch needs.  POD, passed by value.
@@ -47,7 +48,7 @@ struct PassArgs {
     int ep_n[4];
     int ep_half[4];
     double ep_kscale[4];
-    double ep_scale, ep_sign, ep_gauss;
+    double ep_scale, ep_sign, ep_gauss, ep_hw;
 };
 
 struct PassKernelInfo {

@@ -18,6 +18,7 @@ namespace fftb {
 template <typename R> __device__ __forceinline__ R ep_factor(const PassArgs &a, int p, const int *bidx)
 {
     R k2 = R(0);
+    R hw = R(1);
 #pragma unroll 4
     for (int ax = 0; ax < a.ep_naxes; ++ax) {
         const int src = a.ep_src[ax];
@@ -26,8 +27,10 @@ template <typename R> __device__ __forceinline__ R ep_factor(const PassArgs &a, 
         const int k = a.ep_half[ax] ? i : (i <= n / 2 ? i : i - n);
         const R kk = R(k) * R(a.ep_kscale[ax]);
         k2 += kk * kk;
+        if (a.ep_half[ax] && i != 0 && 2 * i != n) hw = R(a.ep_hw);
     }
     R f = R(a.ep_scale);
+    if (a.ep_mode & EP_HALFW) f *= hw;
     if (a.ep_mode & EP_POISSON) f = (k2 == R(0)) ? R(0) : f * R(a.ep_sign) / k2;
     if (a.ep_mode & EP_GAUSS) f *= exp(-k2 * R(a.ep_gauss));
     return f;

@@ -137,6 +137,18 @@ int fftb_ffts_poisson(fftb_ffts obj, const void *rhs, void *solution, double sig
  * G(k) = exp(-|k|^2 / (2 sigma^2)); optionally followed in the same fused pass by
  * the Poisson multiply (poisson_sign = 0 disables it). */
 int fftb_ffts_filter(fftb_ffts obj, const void *in, void *out, double sigma, double poisson_sign);
+/* Adjoint kernels for reverse-mode differentiation (no counterpart in the reference).
+ * Treat the half spectrum Y as independent complex variables with gradient
+ * G = dL/dRe(Y) + i dL/dIm(Y).
+ * fftb_ffts_forward_adjoint: the transpose of fftb_ffts_forward, dL/dx = C2R(W G), W = 1/2
+ *   on interior bins of the half axis (1 on its DC and Nyquist bins), unnormalised;
+ *   grad_spectrum may be overwritten.
+ * fftb_ffts_backward_adjoint: the transpose of fftb_ffts_backward (unnormalised C2R),
+ *   G = W2 R2C(dL/dx), W2 = 2 on interior half-axis bins, 1 on DC / Nyquist.
+ * The spectral multiplies and the Poisson / filter round trips are real diagonal in k and
+ * therefore self-adjoint: their adjoint is the same call. */
+int fftb_ffts_forward_adjoint(fftb_ffts obj, void *grad_spectrum, void *grad_real);
+int fftb_ffts_backward_adjoint(fftb_ffts obj, const void *grad_real, void *grad_spectrum);
 /* In-place spectral multiplies on a spectrum in this object's layout (the
  * reference's standalone functors): Poisson sign/|k|^2 (k=0 -> 0) with an extra
  * scale, examples/poisson/source/poisson_periodic_{3d,4d}_autotuned.cpp. */
