@@ -21,6 +21,9 @@ EXPORTS = [
     "fftb_ffts_backward_normalized", "fftb_ffts_poisson", "fftb_ffts_filter", "fftb_ffts_spectrum_poisson",
     "fftb_ffts_num_launches", "fftb_ffts_timing_enable", "fftb_ffts_timing_read",
     "fftb_poisson3d_f32_noalloc", "fftb_ffts_forward_adjoint", "fftb_ffts_backward_adjoint",
+    "fftb_batch_create", "fftb_batch_destroy", "fftb_batch_layout", "fftb_batch_work_size",
+    "fftb_batch_set_work_area", "fftb_batch_set_stream", "fftb_batch_set_tuning", "fftb_batch_exec",
+    "fftb_batch_status", "fftb_batch_describe",
 ]
 
 _lib = None
@@ -69,6 +72,16 @@ def load():
     L.fftb_ffts_timing_enable.argtypes = [c_vp, c_int]
     L.fftb_ffts_timing_read.argtypes = [c_vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(c_d),
                                         ctypes.c_char_p, c_int, c_int, ip]
+    L.fftb_batch_create.argtypes = [c_int, c_int, llp, ctypes.POINTER(c_vp)]
+    L.fftb_batch_destroy.argtypes = [c_vp]
+    L.fftb_batch_layout.argtypes = [c_vp, llp, llp, llp, llp]
+    L.fftb_batch_work_size.argtypes = [c_vp, szp]
+    L.fftb_batch_set_work_area.argtypes = [c_vp, c_vp]
+    L.fftb_batch_set_stream.argtypes = [c_vp, c_vp]
+    L.fftb_batch_set_tuning.argtypes = [c_vp, c_int, c_int]
+    L.fftb_batch_exec.argtypes = [c_vp, c_int, c_vp, c_vp, c_d, c_int]
+    L.fftb_batch_status.argtypes = [c_vp, c_int, ip]
+    L.fftb_batch_describe.argtypes = [c_vp, c_int, c_d, ip, ip, ip, ip]
     L.fftb_ffts_forward_adjoint.argtypes = [c_vp, c_vp, c_vp]
     L.fftb_ffts_backward_adjoint.argtypes = [c_vp, c_vp, c_vp]
     L.fftb_poisson3d_f32_noalloc.argtypes = [c_vp, c_vp, c_ll, c_ll, c_ll, c_d, c_vp]

@@ -1,0 +1,521 @@
+// fftb_batch.cu -- many 3D transforms of uneven sizes in one persistent launch.
+//
+// Every transform of the batch is compiled into its pass program (the same passes
+// as a single ffts object).  The passes of all transforms are flattened into one
+// work list of (pass, tile) items ordered stage by stage: first every tile of the
+// first pass of every transform, then every tile of the second passes, and so on.
+// A persistent kernel (one or more CTAs per SM) takes items from the head of that
+// list with an atomic counter; before working on a tile of pass p it waits until
+// every tile of the previous pass of the same transform has been counted done.
+// Because items are taken in list order, every item a CTA waits for has already
+// been taken by a running CTA that waits only on items earlier still, so the wait
+// always ends; it is nevertheless bounded (FFTB_BATCH_SPIN_LIMIT polls), after
+// which the kernel raises an error flag that fftb_batch_status reports and every
+// CTA returns.  The launch (counter reset + kernel) is captured once into a CUDA
+// graph per buffer binding and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/fftb.h"
+#include "fftb_engine.h"
+#include "fftb_pass.cuh"
+
+namespace fftb {
+namespace {
+
+constexpr int kBatchThreads = 256;
+constexpr long long kSpinLimit = 1LL << 22;  // ~0.5 s of polling at most
+
+struct BatchItem {
+    int pass;
+    int tile;
+};
+
+// buffer binding of one pass: 0 in, 1 out, 2 work
+struct PassBind {
+    int in_buf, out_buf;
+    long long in_off, out_off;  // bytes
+    int nf;
+};
+
+__device__ __forceinline__ int ld_acquire(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+#define FFTB_BATCH_NF_LIST(X) X(8) X(12) X(16) X(20) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(256)
+
+// One tile of a pass of line length NF; not inlined, so every length keeps its own
+// register allocation instead of the union of all of them.
+template <int NF> __device__ __noinline__ void batch_tile(const PassArgs *a, long long line0, unsigned char *smem)
+{
+    pass_body<float, NF, true>(*a, line0, smem);
+}
+
+// ctl[0]: queue head, ctl[1]: error flag, ctl[2 + p]: finished tiles of pass p
+__global__ void __launch_bounds__(kBatchThreads)
+    batch_persistent_kernel(const BatchItem *__restrict__ items, int nitems, const PassArgs *__restrict__ passes,
+                            const PassBind *__restrict__ binds, const int *__restrict__ deps,
+                            const int *__restrict__ ntiles, int *ctl, const void *in, void *out, void *work)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_item, s_ok;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int it = atomicAdd(&ctl[0], 1);
+            int ok = 1;
+            if (it < nitems) {
+                const int dp = deps[items[it].pass];
+                if (dp >= 0) {
+                    const int need = ntiles[dp];
+                    long long k = 0;
+                    while (ld_acquire(&ctl[2 + dp]) < need) {
+                        if (ld_acquire(&ctl[1]) != 0) { ok = 0; break; }
+                        if (++k > kSpinLimit) {
+                            atomicExch(&ctl[1], 1);
+                            ok = 0;
+                            break;
+                        }
+                        __nanosleep(128);
+                    }
+                }
+            }
+            s_item = it;
+            s_ok = ok;
+        }
+        __syncthreads();
+        const int it = s_item;
+        const int ok = s_ok;
+        __syncthreads();
+        if (it >= nitems || !ok) break;
+        const BatchItem bi = items[it];
+        PassArgs a = passes[bi.pass];
+        const PassBind b = binds[bi.pass];
+        const void *bufs[3] = {in, out, work};
+        a.in = (const char *)bufs[b.in_buf] + b.in_off;
+        a.out = (char *)bufs[b.out_buf] + b.out_off;
+        const long long line0 = (long long)bi.tile * a.G;
+        switch (b.nf) {
+#define FFTB_CASE(n)                                                                                                  \
+    case n:                                                                                                           \
+        batch_tile<n>(&a, line0, smem_raw);                                                                           \
+        break;
+            FFTB_BATCH_NF_LIST(FFTB_CASE)
+#undef FFTB_CASE
+        default:
+            break;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(&ctl[2 + bi.pass], 1);
+        }
+    }
+}
+
+bool batch_nf_supported(int nf)
+{
+    switch (nf) {
+#define FFTB_CASE(n) case n:
+        FFTB_BATCH_NF_LIST(FFTB_CASE)
+#undef FFTB_CASE
+        return true;
+    default:
+        return false;
+    }
+}
+
+int floor_pow2(int v)
+{
+    int p = 1;
+    while (p * 2 <= v) p *= 2;
+    return p;
+}
+
+enum BatchOp { OP_FORWARD = 0, OP_BACKWARD = 1, OP_ROUNDTRIP = 2, OP_POISSON = 3, OP_COUNT = 4 };
+
+struct OpPlan {
+    bool built = false;
+    double sign = 0.0;               // Poisson sign the plan was built for
+    Program seq;                     // every pass of every transform, in transform order
+    int npasses = 0, nitems = 0, nstages = 0;
+    size_t smem = 0;
+    void *blob = nullptr;            // device: items, passes, binds, deps, ntiles
+    BatchItem *d_items = nullptr;
+    PassArgs *d_passes = nullptr;
+    PassBind *d_binds = nullptr;
+    int *d_deps = nullptr, *d_ntiles = nullptr;
+    int *d_ctl = nullptr;
+    int grid = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    const void *g_in = nullptr;
+    void *g_out = nullptr, *g_work = nullptr;
+    bool persistent_ok = false;
+};
+
+} // namespace
+} // namespace fftb
+
+using namespace fftb;
+
+struct fftb_batch_s {
+    int dtype = 0, count = 0;
+    std::vector<long long> dims;              // nx, ny, nz per transform
+    std::vector<long long> roff, soff;        // element offsets into the packed real / spectrum arrays
+    long long rtotal = 0, stotal = 0;
+    OpPlan ops[OP_COUNT];
+    void *work = nullptr;
+    bool own_work = false;
+    cudaStream_t stream = 0;
+    int tiles_scale = 1;                      // autotune knob: tiles of G/tiles_scale lines
+    int ctas_per_sm = 0;                      // autotune knob: 0 = occupancy limit
+};
+
+namespace {
+
+// The pass list of transform i for op, with buffers: in/out are the packed user
+// arrays, work holds the packed spectrum for the round trip and the Poisson solve.
+int transform_passes(fftb_batch_s *b, int i, int op, double sign, std::vector<AxisPass> &out)
+{
+    const long long nx = b->dims[3 * i], ny = b->dims[3 * i + 1], nz = b->dims[3 * i + 2];
+    const long long nzh = nz / 2 + 1, C3 = ny * nzh;
+    const long long ro = b->roff[i], so = b->soff[i];
+    auto mk = [](int kind, long long n, long long is, long long os, std::vector<Dim> batch, int ib, int ob,
+                 long long ibase, long long obase) {
+        AxisPass p;
+        p.kind = kind;
+        p.n = (int)n;
+        p.is = is;
+        p.os = os;
+        p.batch = std::move(batch);
+        p.in_buf = ib;
+        p.out_buf = ob;
+        p.in_base = ibase;
+        p.out_base = obase;
+        return p;
+    };
+    const double invN = 1.0 / (double)(nx * ny * nz);
+    if (op == OP_FORWARD) {
+        out.push_back(mk(K_R2C, nz, 1, 1, {Dim{ny, nz, nzh, 1}, Dim{nx, ny * nz, C3, 0}}, B_IN, B_OUT, ro, so));
+        out.push_back(mk(K_C2C_FWD, ny, nzh, nzh, {Dim{nzh, 1, 1, 2}, Dim{nx, C3, C3, 0}}, B_OUT, B_OUT, so, so));
+        out.push_back(mk(K_C2C_FWD, nx, C3, C3, {Dim{nzh, 1, 1, 2}, Dim{ny, nzh, nzh, 1}}, B_OUT, B_OUT, so, so));
+    } else if (op == OP_BACKWARD) {
+        out.push_back(mk(K_C2C_INV, nx, C3, C3, {Dim{nzh, 1, 1, 2}, Dim{ny, nzh, nzh, 1}}, B_IN, B_IN, so, so));
+        out.push_back(mk(K_C2C_INV, ny, nzh, nzh, {Dim{nzh, 1, 1, 2}, Dim{nx, C3, C3, 0}}, B_IN, B_IN, so, so));
+        AxisPass c = mk(K_C2R, nz, 1, 1, {Dim{ny, nzh, nz, 1}, Dim{nx, C3, ny * nz, 0}}, B_IN, B_OUT, so, ro);
+        c.ep_mode = EP_SCALE;
+        c.ep_scale = invN;
+        out.push_back(c);
+    } else {
+        out.push_back(mk(K_R2C, nz, 1, 1, {Dim{ny, nz, nzh, 1}, Dim{nx, ny * nz, C3, 0}}, B_IN, B_WORK, ro, so));
+        out.push_back(mk(K_C2C_FWD, ny, nzh, nzh, {Dim{nzh, 1, 1, 2}, Dim{nx, C3, C3, 0}}, B_WORK, B_WORK, so, so));
+        AxisPass s = mk(K_SANDWICH, nx, C3, C3, {Dim{nzh, 1, 1, 2}, Dim{ny, nzh, nzh, 1}}, B_WORK, B_WORK, so, so);
+        s.ep_mode = EP_SCALE | (op == OP_POISSON ? EP_POISSON : 0);
+        s.ep_scale = 1.0;
+        s.ep_sign = sign;
+        s.ep_axes = {EpAxis{1, -1, (int)nx, 0}, EpAxis{0, 1, (int)ny, 0}, EpAxis{0, 2, (int)nz, 1}};
+        out.push_back(s);
+        out.push_back(mk(K_C2C_INV, ny, nzh, nzh, {Dim{nzh, 1, 1, 2}, Dim{nx, C3, C3, 0}}, B_WORK, B_WORK, so, so));
+        AxisPass c = mk(K_C2R, nz, 1, 1, {Dim{ny, nzh, nz, 1}, Dim{nx, C3, ny * nz, 0}}, B_WORK, B_OUT, so, ro);
+        c.ep_mode = EP_SCALE;
+        c.ep_scale = invN;
+        out.push_back(c);
+    }
+    return FFTB_SUCCESS;
+}
+
+void free_plan(OpPlan &p)
+{
+    if (p.gexec) cudaGraphExecDestroy(p.gexec);
+    if (p.graph) cudaGraphDestroy(p.graph);
+    if (p.blob) cudaFree(p.blob);
+    p = OpPlan();
+}
+
+int build_plan(fftb_batch_s *b, int op, double sign)
+{
+    OpPlan &P = b->ops[op];
+    if (P.built && (op != OP_POISSON || P.sign == sign)) return FFTB_SUCCESS;
+    free_plan(P);
+    P.sign = sign;
+    // per-transform programs (the sequential mode runs them as they are)
+    std::vector<std::vector<int>> tpass(b->count);
+    for (int i = 0; i < b->count; ++i) {
+        std::vector<AxisPass> ps;
+        int st = transform_passes(b, i, op, sign, ps);
+        if (st != FFTB_SUCCESS) return st;
+        for (const AxisPass &p : ps) {
+            tpass[i].push_back((int)P.seq.launches.size());
+            if ((st = program_add(P.seq, b->dtype, p)) != FFTB_SUCCESS) return st;
+        }
+    }
+    P.nstages = (int)tpass[0].size();
+    P.npasses = (int)P.seq.launches.size();
+    // persistent form: the same passes with G capped to kBatchThreads threads per tile
+    P.persistent_ok = (b->dtype == FFTB_F32);
+    std::vector<PassArgs> args(P.npasses);
+    std::vector<PassBind> binds(P.npasses);
+    std::vector<int> deps(P.npasses, -1), ntiles(P.npasses, 0);
+    size_t smem = 0;
+    for (int p = 0; p < P.npasses; ++p) {
+        const Launch &L = P.seq.launches[p];
+        PassArgs a = L.args;
+        const int T = L.k.threads_per_line;
+        if (!batch_nf_supported(L.k.nf)) P.persistent_ok = false;
+        int G = std::min(a.G, floor_pow2(std::max(1, kBatchThreads / T)));
+        G = std::max(1, G / b->tiles_scale);
+        a.G = G;
+        int gs = 0;
+        while ((1 << gs) < G) ++gs;
+        a.gshift = gs;
+        a.pair_io = L.pair_candidate ? 1 : 0;  // buffers are 16-byte aligned (checked at execution)
+        const size_t cb = complex_bytes(b->dtype);
+        const size_t sm = (a.tw_smem ? (size_t)a.ntw * cb : 0) + (size_t)G * 32 + (size_t)G * L.k.line_pitch * cb;
+        smem = std::max(smem, sm);
+        args[p] = a;
+        binds[p] = PassBind{L.in_buf, L.out_buf, (long long)L.in_off_bytes, (long long)L.out_off_bytes, L.k.nf};
+        ntiles[p] = (int)((a.nlines + G - 1) / G);
+    }
+    for (int i = 0; i < b->count; ++i)
+        for (int s = 1; s < P.nstages; ++s) deps[tpass[i][s]] = tpass[i][s - 1];
+    std::vector<BatchItem> items;
+    for (int s = 0; s < P.nstages; ++s)
+        for (int i = 0; i < b->count; ++i) {
+            const int p = tpass[i][s];
+            for (int t = 0; t < ntiles[p]; ++t) items.push_back(BatchItem{p, t});
+        }
+    P.nitems = (int)items.size();
+    P.smem = smem;
+    if (P.persistent_ok) {
+        auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+        const size_t s_items = al(items.size() * sizeof(BatchItem)), s_args = al(args.size() * sizeof(PassArgs)),
+                     s_binds = al(binds.size() * sizeof(PassBind)), s_deps = al(deps.size() * sizeof(int)),
+                     s_nt = al(ntiles.size() * sizeof(int)), s_ctl = al((2 + P.npasses) * sizeof(int));
+        const size_t tot = s_items + s_args + s_binds + s_deps + s_nt + s_ctl;
+        cudaError_t e = cudaMalloc(&P.blob, tot);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return FFTB_ERROR_ALLOC;
+        }
+        char *q = (char *)P.blob;
+        P.d_items = (BatchItem *)q; q += s_items;
+        P.d_passes = (PassArgs *)q; q += s_args;
+        P.d_binds = (PassBind *)q; q += s_binds;
+        P.d_deps = (int *)q; q += s_deps;
+        P.d_ntiles = (int *)q; q += s_nt;
+        P.d_ctl = (int *)q;
+        e = cudaMemcpy(P.d_items, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(P.d_passes, args.data(), args.size() * sizeof(PassArgs), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(P.d_binds, binds.data(), binds.size() * sizeof(PassBind), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(P.d_deps, deps.data(), deps.size() * sizeof(int), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(P.d_ntiles, ntiles.data(), ntiles.size() * sizeof(int), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemset(P.d_ctl, 0, (2 + P.npasses) * sizeof(int));
+        if (e != cudaSuccess) return set_status_from_cuda(e);
+        if (smem > 48 * 1024) {
+            e = cudaFuncSetAttribute((const void *)batch_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
+            if (e != cudaSuccess) return set_status_from_cuda(e);
+        }
+        int dev = 0, sms = 0, occ = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void *)batch_persistent_kernel, kBatchThreads,
+                                                          smem);
+        if (e != cudaSuccess) return set_status_from_cuda(e);
+        if (occ < 1) return FFTB_ERROR_UNSUPPORTED_SIZE;
+        const int per = b->ctas_per_sm > 0 ? std::min(b->ctas_per_sm, occ) : occ;
+        P.grid = std::max(1, std::min(sms * per, P.nitems));
+    }
+    P.built = true;
+    return FFTB_SUCCESS;
+}
+
+int launch_persistent(OpPlan &P, const void *in, void *out, void *work, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(P.d_ctl, 0, (2 + P.npasses) * sizeof(int), s);
+    if (e != cudaSuccess) return set_status_from_cuda(e);
+    batch_persistent_kernel<<<P.grid, kBatchThreads, P.smem, s>>>(P.d_items, P.nitems, P.d_passes, P.d_binds,
+                                                                 P.d_deps, P.d_ntiles, P.d_ctl, in, out, work);
+    return set_status_from_cuda(cudaGetLastError());
+}
+
+int ensure_work(fftb_batch_s *b)
+{
+    if (b->work) return FFTB_SUCCESS;
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, (size_t)b->stotal * complex_bytes(b->dtype));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return FFTB_ERROR_ALLOC;
+    }
+    b->work = p;
+    b->own_work = true;
+    return FFTB_SUCCESS;
+}
+
+} // namespace
+
+extern "C" {
+
+int fftb_batch_create(int dtype, int count, const long long *dims, fftb_batch *out)
+{
+    if (!out) return FFTB_ERROR_INVALID_VALUE;
+    *out = nullptr;
+    if ((dtype != FFTB_F32 && dtype != FFTB_F64) || count < 1 || !dims) return FFTB_ERROR_INVALID_VALUE;
+    for (int i = 0; i < 3 * count; ++i)
+        if (dims[i] < 2 || dims[i] > 4096) return FFTB_ERROR_INVALID_VALUE;
+    fftb_batch_s *b = new (std::nothrow) fftb_batch_s();
+    if (!b) return FFTB_ERROR_ALLOC;
+    b->dtype = dtype;
+    b->count = count;
+    b->dims.assign(dims, dims + 3 * count);
+    for (int i = 0; i < count; ++i) {
+        const long long nx = dims[3 * i], ny = dims[3 * i + 1], nz = dims[3 * i + 2];
+        b->roff.push_back(b->rtotal);
+        b->soff.push_back(b->stotal);
+        // keep every transform's arrays 16-byte aligned
+        b->rtotal += (nx * ny * nz + 3) & ~3LL;
+        b->stotal += (nx * ny * (nz / 2 + 1) + 1) & ~1LL;
+    }
+    *out = b;
+    return FFTB_SUCCESS;
+}
+
+int fftb_batch_destroy(fftb_batch b)
+{
+    if (!b) return FFTB_ERROR_INVALID_HANDLE;
+    for (OpPlan &p : b->ops) free_plan(p);
+    if (b->own_work && b->work) cudaFree(b->work);
+    delete b;
+    return FFTB_SUCCESS;
+}
+
+int fftb_batch_layout(fftb_batch b, long long *real_offsets, long long *spectrum_offsets, long long *real_total,
+                      long long *spectrum_total)
+{
+    if (!b) return FFTB_ERROR_INVALID_HANDLE;
+    for (int i = 0; i < b->count; ++i) {
+        if (real_offsets) real_offsets[i] = b->roff[i];
+        if (spectrum_offsets) spectrum_offsets[i] = b->soff[i];
+    }
+    if (real_total) *real_total = b->rtotal;
+    if (spectrum_total) *spectrum_total = b->stotal;
+    return FFTB_SUCCESS;
+}
+
+int fftb_batch_work_size(fftb_batch b, size_t *bytes)
+{
+    if (!b || !bytes) return FFTB_ERROR_INVALID_HANDLE;
+    *bytes = (size_t)b->stotal * complex_bytes(b->dtype);
+    return FFTB_SUCCESS;
+}
+
+int fftb_batch_set_work_area(fftb_batch b, void *work)
+{
+    if (!b) return FFTB_ERROR_INVALID_HANDLE;
+    if ((uintptr_t)work % 256) return FFTB_ERROR_MISALIGNED;
+    if (b->own_work && b->work) cudaFree(b->work);
+    b->own_work = false;
+    b->work = work;
+    for (OpPlan &p : b->ops) p.g_work = nullptr;  // graphs bound to the old area are recaptured
+    return FFTB_SUCCESS;
+}
+
+int fftb_batch_set_stream(fftb_batch b, void *stream)
+{
+    if (!b) return FFTB_ERROR_INVALID_HANDLE;
+    b->stream = (cudaStream_t)stream;
+    return FFTB_SUCCESS;
+}
+
+int fftb_batch_set_tuning(fftb_batch b, int tiles_scale, int ctas_per_sm)
+{
+    if (!b || tiles_scale < 1 || ctas_per_sm < 0) return FFTB_ERROR_INVALID_VALUE;
+    b->tiles_scale = tiles_scale;
+    b->ctas_per_sm = ctas_per_sm;
+    for (OpPlan &p : b->ops) free_plan(p);
+    return FFTB_SUCCESS;
+}
+
+int fftb_batch_exec(fftb_batch b, int op, const void *in, void *out, double sign, int mode)
+{
+    if (!b) return FFTB_ERROR_INVALID_HANDLE;
+    if (op < 0 || op >= OP_COUNT || !in || !out || mode < 0 || mode > 2) return FFTB_ERROR_INVALID_VALUE;
+    int st = build_plan(b, op, sign);
+    if (st != FFTB_SUCCESS) return st;
+    OpPlan &P = b->ops[op];
+    void *work = nullptr;
+    if (op == OP_ROUNDTRIP || op == OP_POISSON) {
+        if ((st = ensure_work(b)) != FFTB_SUCCESS) return st;
+        work = b->work;
+    }
+    if (mode == 0 || !P.persistent_ok) {
+        // one transform after another, each with its own pass launches
+        return program_exec(P.seq, const_cast<void *>(in), out, work, b->stream);
+    }
+    if ((uintptr_t)in % 16 || (uintptr_t)out % 16 || (uintptr_t)work % 16) return FFTB_ERROR_MISALIGNED;
+    if (mode == 1) return launch_persistent(P, in, out, work, b->stream);
+    // mode 2: replay the captured graph (captured on first use of this binding)
+    if (!P.gexec || P.g_in != in || P.g_out != out || P.g_work != work) {
+        if (P.gexec) cudaGraphExecDestroy(P.gexec);
+        if (P.graph) cudaGraphDestroy(P.graph);
+        P.gexec = nullptr;
+        P.graph = nullptr;
+        cudaStream_t cap;
+        cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return set_status_from_cuda(e);
+        e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            st = launch_persistent(P, in, out, work, cap);
+            cudaGraph_t g = nullptr;
+            e = cudaStreamEndCapture(cap, &g);
+            if (st == FFTB_SUCCESS && e == cudaSuccess) {
+                P.graph = g;
+                e = cudaGraphInstantiate(&P.gexec, g, 0);
+            }
+        }
+        cudaStreamDestroy(cap);
+        if (st != FFTB_SUCCESS) return st;
+        if (e != cudaSuccess) return set_status_from_cuda(e);
+        P.g_in = in;
+        P.g_out = out;
+        P.g_work = work;
+    }
+    return set_status_from_cuda(cudaGraphLaunch(P.gexec, b->stream));
+}
+
+int fftb_batch_status(fftb_batch b, int op, int *error_flag)
+{
+    if (!b || !error_flag || op < 0 || op >= OP_COUNT) return FFTB_ERROR_INVALID_HANDLE;
+    *error_flag = 0;
+    OpPlan &P = b->ops[op];
+    if (!P.built || !P.persistent_ok) return FFTB_SUCCESS;
+    int v = 0;
+    cudaError_t e = cudaMemcpy(&v, P.d_ctl + 1, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return set_status_from_cuda(e);
+    *error_flag = v;
+    return FFTB_SUCCESS;
+}
+
+int fftb_batch_describe(fftb_batch b, int op, double sign, int *passes, int *items, int *grid, int *persistent)
+{
+    if (!b || op < 0 || op >= OP_COUNT) return FFTB_ERROR_INVALID_HANDLE;
+    int st = build_plan(b, op, sign);
+    if (st != FFTB_SUCCESS) return st;
+    const OpPlan &P = b->ops[op];
+    if (passes) *passes = P.npasses;
+    if (items) *items = P.nitems;
+    if (grid) *grid = P.grid;
+    if (persistent) *persistent = P.persistent_ok ? 1 : 0;
+    return FFTB_SUCCESS;
+}
+
+} // extern "C"

@@ -318,7 +318,7 @@ template <int SIGN, int RAD, typename C, typename R> __device__ __forceinline__ 
 // w_{Ns*R}^{(b mod Ns)*r}, runs a radix-R DFT and writes s[(b/Ns)*Ns*R + b%Ns + r*Ns].
 // tw holds the forward roots of length NT (NT a multiple of NF).
 template <typename R, int NF, int SIGN, int PASS, int T>
-__device__ __forceinline__ void stockham_pass(cpx<R> *s, const cpx<R> *tw, int NT, int t)
+__device__ __forceinline__ void stockham_pass(cpx<R> *s, const cpx<R> *tw, int NT, int t, bool act)
 {
     using C = cpx<R>;
     constexpr int RAD = radix_at(NF, PASS);
@@ -329,7 +329,7 @@ __device__ __forceinline__ void stockham_pass(cpx<R> *s, const cpx<R> *tw, int N
 #pragma unroll
     for (int k = 0; k < PER; ++k) {
         const int b = t + k * T;
-        if (PER * T == NB || b < NB) {
+        if (act && (PER * T == NB || b < NB)) {
 #pragma unroll
             for (int r = 0; r < RAD; ++r) v[k][r] = s[pad16(b + r * NB)];
         }
@@ -338,7 +338,7 @@ __device__ __forceinline__ void stockham_pass(cpx<R> *s, const cpx<R> *tw, int N
 #pragma unroll
     for (int k = 0; k < PER; ++k) {
         const int b = t + k * T;
-        if (PER * T == NB || b < NB) {
+        if (act && (PER * T == NB || b < NB)) {
             if constexpr (NS > 1) {
                 const int j = b % NS;
                 const int step = (NT / (NS * RAD)) * j;
@@ -358,21 +358,38 @@ __device__ __forceinline__ void stockham_pass(cpx<R> *s, const cpx<R> *tw, int N
 }
 
 template <typename R, int NF, int SIGN, int PASS, int T>
-__device__ __forceinline__ void stockham_from(cpx<R> *s, const cpx<R> *tw, int NT, int t)
+__device__ __forceinline__ void stockham_from(cpx<R> *s, const cpx<R> *tw, int NT, int t, bool act)
 {
     if constexpr (PASS < num_passes(NF)) {
-        stockham_pass<R, NF, SIGN, PASS, T>(s, tw, NT, t);
-        stockham_from<R, NF, SIGN, PASS + 1, T>(s, tw, NT, t);
+        stockham_pass<R, NF, SIGN, PASS, T>(s, tw, NT, t, act);
+        stockham_from<R, NF, SIGN, PASS + 1, T>(s, tw, NT, t, act);
     }
 }
 
 // Full in-order FFT of length NF on the padded line s by T = threads_per_line(NF)
 // threads (t in [0,T)).  Every thread of the block must call it (it synchronises
-// the block), also those whose line is past the end of the batch.
+// the block); threads with act == false (no line of their own) only join the barriers.
 template <typename R, int NF, int SIGN>
-__device__ __forceinline__ void fft_line(cpx<R> *s, const cpx<R> *tw, int NT, int t)
+__device__ __forceinline__ void fft_line(cpx<R> *s, const cpx<R> *tw, int NT, int t, bool act = true)
 {
-    stockham_from<R, NF, SIGN, 0, threads_per_line(NF)>(s, tw, NT, t);
+    stockham_from<R, NF, SIGN, 0, threads_per_line(NF)>(s, tw, NT, t, act);
+}
+
+// Global -> shared staging of BYTES (4, 8 or 16) bytes.  CG = false: asynchronous
+// cp.async (completed by cp_async_wait_all); CG = true: a synchronous load that
+// bypasses L1 (ld.global.cg), for data other CTAs of the same launch wrote.
+template <bool CG, int BYTES> __device__ __forceinline__ void stage_load(void *d, const void *s, bool ok)
+{
+    if constexpr (!CG) {
+        cp_async<BYTES>(d, s, ok);
+    } else if constexpr (BYTES == 4) {
+        *reinterpret_cast<float *>(d) = ok ? __ldcg(reinterpret_cast<const float *>(s)) : 0.f;
+    } else if constexpr (BYTES == 8) {
+        *reinterpret_cast<float2 *>(d) = ok ? __ldcg(reinterpret_cast<const float2 *>(s)) : make_float2(0.f, 0.f);
+    } else {
+        *reinterpret_cast<float4 *>(d) =
+            ok ? __ldcg(reinterpret_cast<const float4 *>(s)) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
 }
 
 } // namespace fftb

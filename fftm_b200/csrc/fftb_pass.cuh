@@ -36,13 +36,14 @@ template <typename R> __device__ __forceinline__ R ep_factor(const PassArgs &a, 
     return f;
 }
 
-template <typename R, int NF>
-__global__ void __launch_bounds__(512) fftb_pass_kernel(PassArgs a)
+// One CTA's share of a pass: the G lines starting at line0.  Any block size works;
+// threads past G * threads_per_line(NF) only join the barriers.
+template <typename R, int NF, bool CG>
+__device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, unsigned char *smem_raw)
 {
     using C = cpx<R>;
     constexpr int T = threads_per_line(NF);
     constexpr int LP = pad16(NF) + 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     C *stw_s = reinterpret_cast<C *>(smem_raw);
     const int ntw_s = a.tw_smem ? a.ntw : 0;
     long long *offs = reinterpret_cast<long long *>(stw_s + ntw_s);  // [G][2] in/out offsets
@@ -54,7 +55,6 @@ __global__ void __launch_bounds__(512) fftb_pass_kernel(PassArgs a)
     const int gshift = a.gshift;
     const int g = tid / T;
     const int t = tid - g * T;
-    const long long line0 = (long long)blockIdx.x * G;
 
     const C *twg = reinterpret_cast<const C *>(a.tw);
     for (int i = tid; i < ntw_s; i += blockDim.x) stw_s[i] = twg[i];
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(512) fftb_pass_kernel(PassArgs a)
             if (a.in_pts_fast) { gg = e / NF; p = e - gg * NF; }
             else { gg = e & (G - 1); p = e >> gshift; }
             const bool ok = bidx[4 * gg + 3] != 0;
-            cp_async<sizeof(C)>(&lines[gg * LP + pad16(p)], ok ? (const void *)(in + offs[2 * gg] + p * is) : gdummy,
+            stage_load<CG, sizeof(C)>(&lines[gg * LP + pad16(p)], ok ? (const void *)(in + offs[2 * gg] + p * is) : gdummy,
                                 ok);
         }
     } else if (kind == K_R2C) {
@@ -111,13 +111,13 @@ __global__ void __launch_bounds__(512) fftb_pass_kernel(PassArgs a)
             const R *src = in + offs[2 * gg];
             if (a.half) {
                 if (a.pair_io) {
-                    cp_async<sizeof(C)>(dst, ok ? (const void *)(src + 2 * p) : gdummy, ok);
+                    stage_load<CG, sizeof(C)>(dst, ok ? (const void *)(src + 2 * p) : gdummy, ok);
                 } else {
-                    cp_async<sizeof(R)>(&dst->x, ok ? (const void *)(src + (2 * p) * is) : gdummy, ok);
-                    cp_async<sizeof(R)>(&dst->y, ok ? (const void *)(src + (2 * p + 1) * is) : gdummy, ok);
+                    stage_load<CG, sizeof(R)>(&dst->x, ok ? (const void *)(src + (2 * p) * is) : gdummy, ok);
+                    stage_load<CG, sizeof(R)>(&dst->y, ok ? (const void *)(src + (2 * p + 1) * is) : gdummy, ok);
                 }
             } else {
-                cp_async<sizeof(R)>(&dst->x, ok ? (const void *)(src + p * is) : gdummy, ok);
+                stage_load<CG, sizeof(R)>(&dst->x, ok ? (const void *)(src + p * is) : gdummy, ok);
                 dst->y = R(0);
             }
         }
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(512) fftb_pass_kernel(PassArgs a)
             if (a.in_pts_fast) { gg = e / nin; p = e - gg * nin; }
             else { gg = e & (G - 1); p = e >> gshift; }
             const bool ok = bidx[4 * gg + 3] != 0;
-            cp_async<sizeof(C)>(&lines[gg * LP + pad16(p)], ok ? (const void *)(in + offs[2 * gg] + p * is) : gdummy,
+            stage_load<CG, sizeof(C)>(&lines[gg * LP + pad16(p)], ok ? (const void *)(in + offs[2 * gg] + p * is) : gdummy,
                                 ok);
         }
     }
@@ -169,11 +169,11 @@ __global__ void __launch_bounds__(512) fftb_pass_kernel(PassArgs a)
     }
 
     // ------------------------------------------------------------ FFT core
-    C *lnp = active_thread ? ln : lines;  // idle threads of a short last CTA still join the barriers
+    C *lnp = active_thread ? ln : lines;  // threads without a line still join the barriers
     if (kind == K_C2C_INV || kind == K_C2R) {
-        fft_line<R, NF, +1>(lnp, stw, a.ntw, active_thread ? t : 0);
+        fft_line<R, NF, +1>(lnp, stw, a.ntw, active_thread ? t : 0, active_thread);
     } else {
-        fft_line<R, NF, -1>(lnp, stw, a.ntw, active_thread ? t : 0);
+        fft_line<R, NF, -1>(lnp, stw, a.ntw, active_thread ? t : 0, active_thread);
     }
 
     if (kind == K_SANDWICH) {
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(512) fftb_pass_kernel(PassArgs a)
             for (int p = t; p < NF; p += T) ln[pad16(p)] = cscale(ln[pad16(p)], ep_factor<R>(a, p, bidx + 4 * g));
         }
         __syncthreads();
-        fft_line<R, NF, +1>(lnp, stw, a.ntw, active_thread ? t : 0);
+        fft_line<R, NF, +1>(lnp, stw, a.ntw, active_thread ? t : 0, active_thread);
     }
 
     // ------------------------------------------------------------ R2C post-processing
@@ -246,6 +246,13 @@ __global__ void __launch_bounds__(512) fftb_pass_kernel(PassArgs a)
             out[offs[2 * gg + 1] + p * os] = v;
         }
     }
+}
+
+template <typename R, int NF>
+__global__ void __launch_bounds__(512) fftb_pass_kernel(PassArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pass_body<R, NF, false>(a, (long long)blockIdx.x * a.G, smem_raw);
 }
 
 template <typename R, int NF> inline PassKernelInfo pass_kernel_info()

@@ -167,6 +167,40 @@ int fftb_ffts_timing_enable(fftb_ffts obj, int max_launches);
 int fftb_ffts_timing_read(fftb_ffts obj, float *ms, double *bytes, char *names, int name_stride, int cap,
                           int *count);
 
+/* ------------------------------------------------------------------ batched uneven 3D transforms */
+/* Many independent 3D R2C / C2R transforms of different sizes (no counterpart in the
+ * reference, whose ffts holds one size).  Transform i has real shape dims[3i..3i+2] =
+ * (nx, ny, nz) in the ffts layouts; the user's arrays pack the transforms back to back
+ * at the element offsets fftb_batch_layout returns (16-byte aligned).  The passes of
+ * all transforms run either one transform after another (mode 0, plain launches) or
+ * in ONE persistent launch that takes (pass, tile) items from a stage-ordered work
+ * list with per-pass completion counters (mode 1), replayed from a CUDA graph captured
+ * per buffer binding (mode 2).  Persistent modes are float32; float64 batches run mode 0. */
+typedef struct fftb_batch_s *fftb_batch;
+#define FFTB_BATCH_FORWARD 0   /* in: packed real, out: packed spectrum */
+#define FFTB_BATCH_BACKWARD 1  /* in: packed spectrum (overwritten), out: packed real, 1/N scaled */
+#define FFTB_BATCH_ROUNDTRIP 2 /* in, out: packed real; C2R(R2C(x)) / N, spectrum in the work area */
+#define FFTB_BATCH_POISSON 3   /* in: packed right-hand sides, out: solutions (sign as in fftb_ffts_poisson) */
+int fftb_batch_create(int dtype, int count, const long long *dims, fftb_batch *batch);
+int fftb_batch_destroy(fftb_batch batch);
+/* per-transform element offsets (count entries each; may be NULL) and the packed totals */
+int fftb_batch_layout(fftb_batch batch, long long *real_offsets, long long *spectrum_offsets,
+                      long long *real_total, long long *spectrum_total);
+int fftb_batch_work_size(fftb_batch batch, size_t *bytes);
+int fftb_batch_set_work_area(fftb_batch batch, void *work);
+int fftb_batch_set_stream(fftb_batch batch, void *stream);
+/* Tuning knobs chosen by the autotuner: tiles of (default lines)/tiles_scale lines and
+ * at most ctas_per_sm persistent CTAs per SM (0: the occupancy limit). */
+int fftb_batch_set_tuning(fftb_batch batch, int tiles_scale, int ctas_per_sm);
+/* op: FFTB_BATCH_*; sign: Poisson sign (ignored otherwise); mode: 0 sequential plain
+ * launches, 1 one persistent launch, 2 persistent launch replayed from a CUDA graph. */
+int fftb_batch_exec(fftb_batch batch, int op, const void *in, void *out, double sign, int mode);
+/* error flag of the last persistent launch of op: 1 if a dependency wait ran out its
+ * bounded number of polls (the launch then returned early); synchronises the device. */
+int fftb_batch_status(fftb_batch batch, int op, int *error_flag);
+int fftb_batch_describe(fftb_batch batch, int op, double sign, int *passes, int *items, int *grid,
+                        int *persistent);
+
 /* ------------------------------------------------------------------ allocation-free entry point */
 /* Bytes of the spectrum scratch that fftb_poisson3d_f32_noalloc keeps in static
  * device memory (nx * ny * (nz/2+1) * 8 must not exceed it). */

@@ -1,0 +1,106 @@
+"""GPU tests of the batched uneven 3D transforms: every transform of a batch drawn
+like the batched workload (axes from {32, 48, 64, 96, 128}, default_rng(2)) against
+the FP64 oracle, the persistent and graph-replayed launches against the sequential
+one, and the error flag of the bounded dependency waits."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 2e-6
+
+
+@pytest.fixture(scope="module")
+def B(torch_cuda):
+    from fftm_b200 import build
+    build.build()
+    import fftm_b200.batch as B
+    return B
+
+
+def _fill(torch, b, seed):
+    rng = np.random.default_rng(seed)
+    host = np.zeros(b.real_total, np.float32)
+    for i, (nx, ny, nz) in enumerate(b.shapes):
+        o = b.real_offsets[i]
+        host[o:o + nx * ny * nz] = rng.uniform(-1, 1, nx * ny * nz)
+    return torch.tensor(host, device="cuda"), host
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_batch_forward_backward_vs_oracle(B, torch_cuda, mode):
+    torch = torch_cuda
+    shapes = B.draw_shapes(12, seed=2)
+    b = B.Batch(shapes)
+    x, host = _fill(torch, b, 5)
+    spec = torch.zeros(b.spectrum_total, dtype=torch.complex64, device="cuda")
+    b.exec(B.FORWARD, x, spec, mode=mode)
+    torch.cuda.synchronize()
+    assert b.status(B.FORWARD) == 0
+    sp = spec.cpu().numpy().astype(np.complex128)
+    for i, s in enumerate(shapes):
+        o = b.real_offsets[i]
+        xi = host[o:o + np.prod(s)].reshape(s).astype(np.float64)
+        so = b.spectrum_offsets[i]
+        got = sp[so:so + s[0] * s[1] * (s[2] // 2 + 1)].reshape(s[0], s[1], s[2] // 2 + 1)
+        assert O.rel_l2(got, O.ffts3d_forward(xi)) <= TOL, (i, s)
+    out = torch.zeros_like(x)
+    b.exec(B.BACKWARD, spec, out, mode=mode)
+    torch.cuda.synchronize()
+    res = out.cpu().numpy().astype(np.float64)
+    for i, s in enumerate(shapes):
+        o = b.real_offsets[i]
+        n = int(np.prod(s))
+        assert O.rel_l2(res[o:o + n], host[o:o + n].astype(np.float64)) <= TOL, (i, s)
+
+
+def test_batch_roundtrip_poisson_modes_agree(B, torch_cuda):
+    torch = torch_cuda
+    shapes = B.draw_shapes(40, seed=2)
+    b = B.Batch(shapes)
+    x, host = _fill(torch, b, 6)
+    outs = {}
+    for op in (B.ROUNDTRIP, B.POISSON):
+        for mode in (0, 1, 2):
+            out = torch.zeros_like(x)
+            b.exec(op, x, out, sign=-1.0, mode=mode)
+            b.exec(op, x, out, sign=-1.0, mode=mode)   # replay the same binding
+            torch.cuda.synchronize()
+            assert b.status(op) == 0
+            outs[(op, mode)] = out.cpu().numpy()
+        # the same per-line arithmetic in every mode
+        np.testing.assert_array_equal(outs[(op, 0)], outs[(op, 1)])
+        np.testing.assert_array_equal(outs[(op, 0)], outs[(op, 2)])
+    rt = outs[(B.ROUNDTRIP, 2)].astype(np.float64)
+    assert O.rel_l2(rt, host.astype(np.float64)) <= TOL
+    po = outs[(B.POISSON, 2)].astype(np.float64)
+    for i in (0, 7, 21, 39):
+        s = shapes[i]
+        o = b.real_offsets[i]
+        n = int(np.prod(s))
+        ref = O.poisson3d_solve(host[o:o + n].reshape(s).astype(np.float64), -1.0)
+        assert O.rel_l2(po[o:o + n].reshape(s), ref) <= TOL
+
+
+def test_batch_full_workload_512(B, torch_cuda):
+    torch = torch_cuda
+    shapes = B.draw_shapes(512, seed=2)
+    b = B.Batch(shapes)
+    d = b.describe(B.ROUNDTRIP)
+    assert d["persistent"] == 1 and d["passes"] == 5 * 512
+    x, host = _fill(torch, b, 7)
+    out = torch.zeros_like(x)
+    b.exec(B.ROUNDTRIP, x, out, mode=2)
+    torch.cuda.synchronize()
+    assert b.status(B.ROUNDTRIP) == 0
+    assert float(torch.linalg.norm(out - x) / torch.linalg.norm(x)) <= TOL
+
+
+def test_partition_lpt_balances():
+    import fftm_b200.batch as B
+    shapes = B.draw_shapes(512, seed=2)
+    parts = B.partition_lpt(shapes, 4)
+    assert sorted(i for p in parts for i in p) == list(range(512))
+    loads = [sum(B.transform_bytes(shapes[i]) for i in p) for p in parts]
+    assert max(loads) / min(loads) < 1.01
