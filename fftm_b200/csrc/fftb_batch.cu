@@ -53,10 +53,12 @@ __device__ __forceinline__ int ld_acquire(const int *p)
 #define FFTB_BATCH_NF_LIST(X) X(8) X(12) X(16) X(20) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(256)
 
 // One tile of a pass of line length NF; not inlined, so every length keeps its own
-// register allocation instead of the union of all of them.
+// register allocation instead of the union of all of them.  The tile stages its lines
+// with cp.async: thread 0's acquire load of the producer counters followed by the
+// CTA barrier orders these loads after the producers' fenced stores (PTX memory model).
 template <int NF> __device__ __noinline__ void batch_tile(const PassArgs *a, long long line0, unsigned char *smem)
 {
-    pass_body<float, NF, true>(*a, line0, smem);
+    pass_body<float, NF, false>(*a, line0, smem);
 }
 
 // ctl[0]: queue head, ctl[1]: error flag, ctl[2 + p]: finished tiles of pass p
