@@ -225,13 +225,9 @@ def main():
         return 0
 
     import torch
+    from fftm_b200 import replicas
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    dist = replicas.init_group("nccl", device=torch.device("cuda", local))
 
     from fftm_b200 import build as _build
     if rank == 0 or world == 1:
@@ -282,11 +278,8 @@ def main():
     total_ms = sum(step_ms)
     per_launch = ff.timing_read()
     ff.timing_enable(0)
-    if dist is not None:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = BYTES_RT * args.steps * world / (total_ms * 1e-3) / 1e9
+    total_ms = replicas.max_over_ranks(dist, total_ms, dev)
+    value = replicas.whole_job_rate(BYTES_RT, args.steps, world, total_ms) / 1e9
 
     # per-kernel roofline from the live per-launch events
     agg = {}
@@ -325,11 +318,8 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_val = BYTES_RT * e2e_steps * world / (e2e_ms * 1e-3) / 1e9
+    e2e_ms = replicas.max_over_ranks(dist, e2e_ms, dev)
+    e2e_val = replicas.whole_job_rate(BYTES_RT, e2e_steps, world, e2e_ms) / 1e9
 
     # secondary size of the metric: 4D 64^4 native_xzwy R2C + C2R round trip (forward, then the
     # normalised inverse), input N(0,1) from default_rng(1), same flush / event protocol
@@ -385,6 +375,63 @@ def main():
     except Exception as exc:  # noqa: BLE001
         sec = {"unavailable": str(exc)[:200]}
 
+    # batched uneven 3D transforms: 512 shapes with every axis drawn from {32, 48, 64, 96, 128}
+    # (numpy default_rng(2)); one step = the R2C + normalised C2R round trip of every transform.
+    # The execution knobs come from the autotuner (fresh cache per run); sequential plain launches
+    # of the same batch are timed beside it.  With N > 1 each rank runs its LPT share.
+    bat = None
+    try:
+        import tempfile
+
+        import fftm_b200.autotune as AT
+        import fftm_b200.batch as B
+        shapes = B.draw_shapes(512, seed=2)
+        mine = [shapes[i] for i in replicas.shard(shapes, rank, world)]
+        bt = B.Batch(mine)
+        gen = torch.Generator(device=dev).manual_seed(2 + rank)
+        bx = torch.rand(bt.real_total, device=dev, generator=gen) * 2 - 1
+        by = torch.empty_like(bx)
+        bbytes = bt.algorithmic_bytes()
+        with tempfile.TemporaryDirectory() as td:
+            sel = bt.autotune(B.ROUNDTRIP, os.path.join(td, "batch.env"),
+                              measured=AT.measured_options(warmup=2, iterations=5))
+
+        def time_batch(mode, n):
+            for _ in range(2):
+                bt.exec(B.ROUNDTRIP, bx, by, mode=mode)
+            torch.cuda.synchronize()
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+            for a, b in evs:
+                flush.zero_()
+                a.record(stream)
+                bt.exec(B.ROUNDTRIP, bx, by, mode=mode)
+                b.record(stream)
+            torch.cuda.synchronize()
+            return sum(a.elapsed_time(b) for a, b in evs)
+
+        if dist is not None:
+            dist.barrier()
+        tuned_ms = replicas.max_over_ranks(dist, time_batch(bt.mode, 10), dev) / 10
+        status = bt.status(B.ROUNDTRIP)
+        berr = float(torch.linalg.norm(by - bx) / torch.linalg.norm(bx))
+        seq_ms = replicas.max_over_ranks(dist, time_batch(B.SEQUENTIAL, 5), dev) / 5
+        total_bytes = sum(B.transform_bytes(s_) for s_ in shapes)
+        bat = {"workload": "512 uneven 3D f32 R2C + normalised C2R round trips, axes from {32,48,64,96,128}, "
+                           "numpy default_rng(2)",
+               "ms_per_step": tuned_ms, "value": total_bytes / (tuned_ms * 1e-3) / 1e9, "unit": "GB/s",
+               "bytes_per_step": total_bytes, "bytes_this_rank": bbytes,
+               "tuned": {k: sel.config.get(k) for k in ("FFTM_AUTOTUNE_STRATEGY_3D", "FFTB_AUTOTUNE_BATCH_MODE",
+                                                       "FFTB_AUTOTUNE_TILES_SCALE", "FFTB_AUTOTUNE_CTAS_PER_SM")},
+               "candidates_median_ms": sel.medians_ms(),
+               "launches_per_step": 1 if bt.mode != B.SEQUENTIAL else bt.describe(B.ROUNDTRIP)["passes"],
+               "wait_error_flag": status, "round_trip_rel_l2": berr,
+               "sequential_plain_launches": {"ms_per_step": seq_ms,
+                                             "value": total_bytes / (seq_ms * 1e-3) / 1e9,
+                                             "launches_per_step": bt.describe(B.ROUNDTRIP)["passes"]}}
+        del bx, by, bt
+    except Exception as exc:  # noqa: BLE001
+        bat = {"unavailable": str(exc)[:200]}
+
     # the same solve through cuFFT (torch.fft: R2C, multiply by -1/|k|^2, C2R with 1/N), the
     # library the reference's ffts wraps, timed with the same flush / event protocol
     cufft = None
@@ -439,6 +486,7 @@ def main():
         "clocks": clk,
         "cufft_same_gpu": cufft,
         "secondary": sec,
+        "batched": bat,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, secs, threads, ref = cpu_oracle_rate(f_host, 1)

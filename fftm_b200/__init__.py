@@ -348,6 +348,40 @@ class ffts:
         _check(_lib.load().fftb_ffts_num_launches(self._h, code, ctypes.byref(v)), "num_launches")
         return v.value
 
+    # ------------------------------------------------------------------ strategy / autotune
+    def set_strategy(self, strategy="auto", plane_cluster=0):
+        """"auto", "fused" (multi-axis kernels; plane_cluster 1, 2 or 4 CTAs per 3D
+        plane, 0 by occupancy) or "staged" (one pass kernel per axis)."""
+        self._ensure()
+        code = {"auto": 0, "fused": 1, "staged": 2}[strategy]
+        _check(_lib.load().fftb_ffts_set_strategy(self._h, code, int(plane_cluster)), "set_strategy")
+
+    def strategy(self):
+        """(strategy in effect, plane cluster size)."""
+        self._ensure()
+        s, c = ctypes.c_int(), ctypes.c_int()
+        _check(_lib.load().fftb_ffts_get_strategy(self._h, ctypes.byref(s), ctypes.byref(c)), "get_strategy")
+        return ("fused" if s.value == 1 else "staged"), c.value
+
+    def apply_config(self, config):
+        """Applies a tuned config (dict or KEY=VALUE text) to this object."""
+        from . import autotune as _at
+        self._ensure()
+        text = config if isinstance(config, str) else _at.to_text(config)
+        _check(_lib.load().fftb_ffts_apply_config(self._h, text.encode()), "apply_config")
+
+    def autotune(self, cache_file, options=None, measured=None):
+        """load_or_measure for this object's problem, then applies the winner; returns
+        the selected config."""
+        from . import autotune as _at
+        self._ensure()
+        opts = options or _at.autotune_options()
+        opts.cache_file = str(cache_file)
+        dt = "float32" if self.dtype == F32 else "float64"
+        sel = _at.load_or_measure_config(dt, self._dims, opts, measured, strategy_4d=self.strategy_4d)
+        self.apply_config(sel.config)
+        return sel
+
     def timing_enable(self, max_launches=4096):
         """Per-launch device timing of later calls (profiling hook)."""
         self._ensure()

@@ -24,6 +24,9 @@ EXPORTS = [
     "fftb_batch_create", "fftb_batch_destroy", "fftb_batch_layout", "fftb_batch_work_size",
     "fftb_batch_set_work_area", "fftb_batch_set_stream", "fftb_batch_set_tuning", "fftb_batch_exec",
     "fftb_batch_status", "fftb_batch_describe",
+    "fftb_ffts_set_strategy", "fftb_ffts_get_strategy",
+    "fftb_autotune_load_file", "fftb_autotune_save_file", "fftb_autotune_validate", "fftb_autotune_hardware",
+    "fftb_autotune_ffts", "fftb_ffts_apply_config", "fftb_autotune_batch", "fftb_batch_apply_config",
 ]
 
 _lib = None
@@ -85,6 +88,17 @@ def load():
     L.fftb_ffts_forward_adjoint.argtypes = [c_vp, c_vp, c_vp]
     L.fftb_ffts_backward_adjoint.argtypes = [c_vp, c_vp, c_vp]
     L.fftb_poisson3d_f32_noalloc.argtypes = [c_vp, c_vp, c_ll, c_ll, c_ll, c_d, c_vp]
+    cp = ctypes.c_char_p
+    L.fftb_ffts_set_strategy.argtypes = [c_vp, c_int, c_int]
+    L.fftb_ffts_get_strategy.argtypes = [c_vp, ip, ip]
+    L.fftb_autotune_load_file.argtypes = [cp, cp, c_sz, szp]
+    L.fftb_autotune_save_file.argtypes = [cp, cp]
+    L.fftb_autotune_validate.argtypes = [cp, cp, c_int]
+    L.fftb_autotune_hardware.argtypes = [c_int, cp, c_sz, szp]
+    L.fftb_autotune_ffts.argtypes = [c_int, c_ll, c_ll, c_ll, c_ll, c_int, cp, c_int, c_int, c_int, cp, c_sz, szp, ip]
+    L.fftb_ffts_apply_config.argtypes = [c_vp, cp]
+    L.fftb_autotune_batch.argtypes = [c_vp, c_int, c_d, cp, c_int, c_int, c_int, cp, c_sz, szp, ip, ip]
+    L.fftb_batch_apply_config.argtypes = [c_vp, cp, ip]
     for name in EXPORTS:
         if name not in ("fftb_status_string", "fftb_version", "fftb_last_error_message"):
             getattr(L, name).restype = c_int

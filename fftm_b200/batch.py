@@ -68,6 +68,7 @@ class Batch:
         self.real_total = rt.value
         self.spectrum_total = st.value
         self._work = None
+        self.mode = GRAPH
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -85,7 +86,30 @@ class Batch:
     def set_tuning(self, tiles_scale=1, ctas_per_sm=0):
         _check(_lib.load().fftb_batch_set_tuning(self._h, int(tiles_scale), int(ctas_per_sm)), "set_tuning")
 
-    def exec(self, op, inp, out, sign=-1.0, mode=GRAPH, stream=None):
+    def apply_config(self, config) -> int:
+        """Applies a tuned config's knobs; returns its execution mode."""
+        from . import autotune as _at
+        text = config if isinstance(config, str) else _at.to_text(config)
+        m = ctypes.c_int()
+        _check(_lib.load().fftb_batch_apply_config(self._h, text.encode(), ctypes.byref(m)), "apply_config")
+        self.mode = m.value
+        return m.value
+
+    def autotune(self, op, cache_file, options=None, measured=None, sign=-1.0):
+        """load_or_measure of the execution mode and tiling for op; the winner is applied
+        and its mode becomes the default of :meth:`exec`.  Returns the selected config."""
+        from . import autotune as _at
+        opts = options or _at.autotune_options()
+        opts.cache_file = str(cache_file)
+        sel, mode = _at.autotune_batch(self, op, opts, measured, sign)
+        self.mode = mode
+        return sel
+
+    def exec(self, op, inp, out, sign=-1.0, mode=None, stream=None):
+        """mode: SEQUENTIAL, PERSISTENT or GRAPH; None takes the tuned mode (GRAPH if the
+        batch was never tuned)."""
+        if mode is None:
+            mode = self.mode
         L = _lib.load()
         _check(L.fftb_batch_set_stream(self._h, _stream_ptr(stream)), "set_stream")
         _check(L.fftb_batch_exec(self._h, int(op), _ptr(inp), _ptr(out), float(sign), int(mode)), "fftb_batch_exec")

@@ -135,6 +135,10 @@ const char *fftb_status_string(int s)
     case FFTB_ERROR_ALREADY_INITIALIZED: return "ffts::init can only be called once per instance.";
     case FFTB_ERROR_MISALIGNED: return "misaligned pointer";
     case FFTB_ERROR_NO_WORK_AREA: return "work area required";
+    case FFTB_ERROR_CACHE_IO: return "autotune cache cannot be read, parsed or written";
+    case FFTB_ERROR_CACHE_MISMATCH: return "autotune cache does not match this problem or hardware";
+    case FFTB_ERROR_CACHE_MISSING: return "autotune cache file does not exist";
+    case FFTB_ERROR_TUNE_FAILED: return "no autotune candidate passed its round-trip check";
     default: return "unknown status";
     }
 }

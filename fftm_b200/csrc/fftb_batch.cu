@@ -365,6 +365,21 @@ int ensure_work(fftb_batch_s *b)
 
 } // namespace
 
+namespace fftb {
+int batch_identity(const fftb_batch_s *b, int *dtype, int *count, const long long **dims, int *tiles_scale,
+                   int *ctas_per_sm, void **stream)
+{
+    if (!b) return FFTB_ERROR_INVALID_HANDLE;
+    *stream = (void *)b->stream;
+    *dtype = b->dtype;
+    *count = b->count;
+    *dims = b->dims.data();
+    *tiles_scale = b->tiles_scale;
+    *ctas_per_sm = b->ctas_per_sm;
+    return FFTB_SUCCESS;
+}
+} // namespace fftb
+
 extern "C" {
 
 int fftb_batch_create(int dtype, int count, const long long *dims, fftb_batch *out)

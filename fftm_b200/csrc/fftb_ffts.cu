@@ -640,4 +640,62 @@ int fftb_ffts_num_launches(fftb_ffts o, int which, int *launches)
     return FFTB_SUCCESS;
 }
 
+int fftb_ffts_set_strategy(fftb_ffts o, int strategy, int plane_cluster)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (strategy < FFTB_STRATEGY_AUTO || strategy > FFTB_STRATEGY_STAGED) return FFTB_ERROR_INVALID_VALUE;
+    if (plane_cluster != 0 && plane_cluster != 1 && plane_cluster != 2 && plane_cluster != 4)
+        return FFTB_ERROR_INVALID_VALUE;
+    if (o->dim == 2) {
+        if (strategy == FFTB_STRATEGY_FUSED) {
+            set_last_error("2D transforms have no fused kernels");
+            return FFTB_ERROR_UNSUPPORTED_SIZE;
+        }
+        return FFTB_SUCCESS;
+    }
+    int st = FFTB_SUCCESS;
+    if (o->dim == 3) {
+        Fused3D f;
+        if (strategy != FFTB_STRATEGY_STAGED)
+            st = fused3d_init(f, o->dtype, o->nx, o->ny, o->nz, plane_cluster);
+        if (st != FFTB_SUCCESS) return st;
+        if (strategy == FFTB_STRATEGY_FUSED && !f.enabled) {
+            set_last_error("no fused 3D kernels for this size / dtype / plane cluster");
+            return FFTB_ERROR_UNSUPPORTED_SIZE;
+        }
+        o->fused = f;
+    } else {
+        Fused4D f;
+        if (plane_cluster > 1) {
+            set_last_error("4D plane kernels run one CTA per plane");
+            return FFTB_ERROR_UNSUPPORTED_SIZE;
+        }
+        if (strategy != FFTB_STRATEGY_STAGED)
+            st = fused4d_init(f, o->dtype, o->layout, o->nx, o->ny, o->nz, o->nw);
+        if (st != FFTB_SUCCESS) return st;
+        if (strategy == FFTB_STRATEGY_FUSED && !f.enabled) {
+            set_last_error("no fused 4D kernels for this size / dtype / layout");
+            return FFTB_ERROR_UNSUPPORTED_SIZE;
+        }
+        o->fused4 = f;
+    }
+    return FFTB_SUCCESS;
+}
+
+int fftb_ffts_get_strategy(fftb_ffts o, int *strategy, int *plane_cluster)
+{
+    if (!o || !strategy || !plane_cluster) return FFTB_ERROR_INVALID_HANDLE;
+    if (o->fused.enabled) {
+        *strategy = FFTB_STRATEGY_FUSED;
+        *plane_cluster = o->fused.cluster;
+    } else if (o->fused4.enabled) {
+        *strategy = FFTB_STRATEGY_FUSED;
+        *plane_cluster = 1;
+    } else {
+        *strategy = FFTB_STRATEGY_STAGED;
+        *plane_cluster = 0;
+    }
+    return FFTB_SUCCESS;
+}
+
 } // extern "C"

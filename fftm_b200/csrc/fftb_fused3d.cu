@@ -665,19 +665,35 @@ int launch_xcol(const Fused3D &f, int mode, void *data, const EpValues *ep, cuda
 
 } // namespace
 
-int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz)
+int fused3d_clusters(int dtype, long long nx, long long ny, long long nz, int *clusters, int cap)
+{
+    int n = 0;
+    if (dtype != FFTB_F32 || !find_xcol(dtype, (int)nx)) return 0;
+    for (int cl = 1; cl <= 4; cl *= 2) {
+        const PlaneEntry *e = find_plane(dtype, (int)ny, (int)nz, cl);
+        if (e && e->smem_fwd <= 227 * 1024 && e->smem_inv <= 227 * 1024 && n < cap) clusters[n++] = cl;
+    }
+    return n;
+}
+
+int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz, int force_cluster)
 {
     f.enabled = false;
     f.dtype = dtype;
     f.nx = nx;
     f.ny = ny;
     f.nz = nz;
+    f.cluster = 0;
     if (dtype != FFTB_F32) return FFTB_SUCCESS;
     if (getenv("FFTB_DISABLE_FUSED3D")) return FFTB_SUCCESS;
+    const PlaneEntry *pe = nullptr;
+    if (force_cluster > 0) {
+        const PlaneEntry *e = find_plane(dtype, (int)ny, (int)nz, force_cluster);
+        if (e && e->smem_fwd <= 227 * 1024 && e->smem_inv <= 227 * 1024) pe = e;
+    }
     // the smallest cluster whose CTAs fit two per SM and whose grid fills two waves;
     // failing that, the smallest one that fits one per SM
-    const PlaneEntry *pe = nullptr;
-    for (int cl = 1; cl <= 4 && !pe; cl *= 2) {
+    for (int cl = 1; cl <= 4 && !pe && force_cluster <= 0; cl *= 2) {
         const PlaneEntry *e = find_plane(dtype, (int)ny, (int)nz, cl);
         if (e && e->smem_fwd <= 113 * 1024 && e->smem_inv <= 113 * 1024 && nx * cl >= 2 * 148) pe = e;
     }
@@ -701,6 +717,7 @@ int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz
     if ((st = engine_roots(dtype, (int)nx, &f.roots_x)) != FFTB_SUCCESS) return st;
     f.plane = pe;
     f.xcol = xe;
+    f.cluster = pe->cl;
     f.enabled = true;
     return FFTB_SUCCESS;
 }

@@ -12,14 +12,19 @@ struct Fused3D {
     bool enabled = false;
     int dtype = 0;
     long long nx = 0, ny = 0, nz = 0;
+    int cluster = 0;               // CTAs per (y, z) plane of the selected plane kernels
     const void *plane = nullptr;   // selected plane kernel entry
     const void *xcol = nullptr;    // selected x column kernel entry
     void *roots_plane = nullptr;   // device root table of length max(ny, nz)
     void *roots_x = nullptr;       // device root table of length nx
 };
 
-// Sets f.enabled when (dtype, nx, ny, nz) has a specialised path.
-int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz);
+// Sets f.enabled when (dtype, nx, ny, nz) has a specialised path.  force_cluster = 0
+// picks the plane cluster size by occupancy; 1, 2 or 4 asks for that size (f stays
+// disabled when the size has no such plane kernel).
+int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz, int force_cluster = 0);
+// The cluster sizes with plane kernels for (dtype, ny, nz) that fit the shared memory of a CTA.
+int fused3d_clusters(int dtype, long long nx, long long ny, long long nz, int *clusters, int cap);
 int fused3d_forward(const Fused3D &f, const void *in, void *out, cudaStream_t s, LaunchTimer *t);
 int fused3d_backward(const Fused3D &f, void *in, void *out, double scale, cudaStream_t s, LaunchTimer *t);
 int fused3d_spectral(const Fused3D &f, const void *in, void *out, void *work, const EpValues &ep, cudaStream_t s,

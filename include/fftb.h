@@ -42,6 +42,10 @@ extern "C" {
 #define FFTB_ERROR_ALREADY_INITIALIZED (-8) /* init twice (source/ffts.hpp:631-637) */
 #define FFTB_ERROR_MISALIGNED (-9)        /* pointer not aligned to its element type */
 #define FFTB_ERROR_NO_WORK_AREA (-10)     /* work area required but missing */
+#define FFTB_ERROR_CACHE_IO (-11)         /* autotune cache unreadable, not KEY=VALUE, or not writable */
+#define FFTB_ERROR_CACHE_MISMATCH (-12)   /* autotune cache for another problem, schema or hardware */
+#define FFTB_ERROR_CACHE_MISSING (-13)    /* autotune cache absent and creation not requested */
+#define FFTB_ERROR_TUNE_FAILED (-14)      /* every autotune candidate failed */
 
 /* direction values equal fftm::direction (source/fft_direction.h:9-15) */
 #define FFTB_R2C 1
@@ -167,6 +171,20 @@ int fftb_ffts_timing_enable(fftb_ffts obj, int max_launches);
 int fftb_ffts_timing_read(fftb_ffts obj, float *ms, double *bytes, char *names, int name_stride, int cap,
                           int *count);
 
+/* Execution strategy of an ffts object (the knob the autotuner below measures; the
+ * role of fftm's FFTM_AUTOTUNE_STRATEGY_3D/_4D choice, source/fftm_autotune.hpp:31-70).
+ *  AUTO    the default: fused multi-axis kernels where the size has them, with the plane
+ *          cluster size picked by occupancy; per-axis pass programs otherwise
+ *  FUSED   fused kernels (FFTB_ERROR_UNSUPPORTED_SIZE when the size has none); for 3D,
+ *          plane_cluster 1, 2 or 4 picks the CTAs per (y, z) plane (0: by occupancy)
+ *  STAGED  one pass kernel per axis (the generic pass programs) */
+#define FFTB_STRATEGY_AUTO 0
+#define FFTB_STRATEGY_FUSED 1
+#define FFTB_STRATEGY_STAGED 2
+int fftb_ffts_set_strategy(fftb_ffts obj, int strategy, int plane_cluster);
+/* the strategy in effect (FUSED or STAGED) and its plane cluster size (0 when STAGED) */
+int fftb_ffts_get_strategy(fftb_ffts obj, int *strategy, int *plane_cluster);
+
 /* ------------------------------------------------------------------ batched uneven 3D transforms */
 /* Many independent 3D R2C / C2R transforms of different sizes (no counterpart in the
  * reference, whose ffts holds one size).  Transform i has real shape dims[3i..3i+2] =
@@ -200,6 +218,55 @@ int fftb_batch_exec(fftb_batch batch, int op, const void *in, void *out, double 
 int fftb_batch_status(fftb_batch batch, int op, int *error_flag);
 int fftb_batch_describe(fftb_batch batch, int op, double sign, int *passes, int *items, int *grid,
                         int *persistent);
+
+/* ------------------------------------------------------------------ autotuner */
+/* The replacement of fftm's autotune surface (source/fftm_autotune.hpp:31-169, 452-477,
+ * 660-676; source/fftm_autotune_measure.hpp:21-55, 432-520, 798-854;
+ * source/detail/fftm_autotune_hardware.inc:285-425) for the single-GPU transforms:
+ * measured candidates, the least median of timed forward+backward pairs (each pair timed
+ * with CUDA events on a private stream after `warmup` untimed pairs; every candidate must
+ * pass a round-trip check at 64 sampled points, tolerance 1000 eps max(1, log2 N)), and
+ * a KEY=VALUE cache file written to <path>.tmp and renamed into place.  The cache carries
+ * fftm's schema-2 identity keys (FFTM_AUTOTUNE_SCHEMA=2, _POLICY_VERSION, _LIBRARY=fftb,
+ * _DIM, _NUM_GPUS=1, _SIZE_2D/_3D/_4D, _SPECTRAL_LAYOUT_4D, _SOURCE), a "v2:" hardware
+ * signature (64-bit FNV-1a of the device class; _STRICT adds UUID and PCI bus id) with
+ * the device metadata keys, and the tuned FFTB_AUTOTUNE_* keys. */
+#define FFTB_TUNE_CREATE_IF_MISSING 1      /* autotune_options::create_if_missing */
+#define FFTB_TUNE_OVERWRITE_ON_MISMATCH 2  /* cache_mismatch_policy::overwrite (else error) */
+#define FFTB_TUNE_NO_HARDWARE_CHECK 4      /* validate_hardware = false */
+#define FFTB_TUNE_STRICT_DEVICE 8          /* strict_device_identity */
+#define FFTB_TUNE_FORCE_MEASURE 16         /* measure and rewrite even if the cache matches */
+/* Reads and parses a cache file; returns its canonical text (sorted KEY=VALUE lines).
+ * *needed receives the bytes the text takes including its NUL; text may be NULL with
+ * capacity 0 to query it.  FFTB_ERROR_CACHE_IO on an unreadable file, an empty file or
+ * a line that is not KEY=VALUE. */
+int fftb_autotune_load_file(const char *path, char *text, size_t capacity, size_t *needed);
+/* Parses KEY=VALUE text and writes it to path through <path>.tmp and rename. */
+int fftb_autotune_save_file(const char *path, const char *text);
+/* Checks a cache against expected identity and hardware keys (the keys present in
+ * expected_text are compared; the cache must also be a measured fftb cache).  Returns
+ * FFTB_ERROR_CACHE_MISMATCH with a message naming the first differing key. */
+int fftb_autotune_validate(const char *cache_text, const char *expected_text, int flags);
+/* The hardware keys (signatures and device metadata) of a CUDA device. */
+int fftb_autotune_hardware(int device, char *text, size_t capacity, size_t *needed);
+/* load_or_measure for an ffts problem (dims and layout4d as fftb_ffts_create) on the
+ * current device: use the cache when it matches; measure when it is missing (with
+ * CREATE_IF_MISSING, else FFTB_ERROR_CACHE_MISSING) or mismatches (with
+ * OVERWRITE_ON_MISMATCH, else FFTB_ERROR_CACHE_MISMATCH).  Returns the config text and
+ * *from_cache = 1 when it came from the file.  Candidates: fused kernels with each
+ * available plane cluster size, and the staged per-axis passes. */
+int fftb_autotune_ffts(int dtype, long long nx, long long ny, long long nz, long long nw, int layout4d,
+                       const char *cache_file, int flags, int warmup, int iterations, char *text, size_t capacity,
+                       size_t *needed, int *from_cache);
+/* Applies the FFTB_AUTOTUNE_STRATEGY / _PLANE_CLUSTER of a config to an ffts object. */
+int fftb_ffts_apply_config(fftb_ffts obj, const char *text);
+/* load_or_measure for a batch and one op: candidates are sequential launches and the
+ * graph-replayed persistent launch with tiles_scale {1, 2} x ctas_per_sm {0, 1, 2}.  The
+ * winner's knobs are applied to the batch and its mode returned in *mode. */
+int fftb_autotune_batch(fftb_batch batch, int op, double sign, const char *cache_file, int flags, int warmup,
+                        int iterations, char *text, size_t capacity, size_t *needed, int *from_cache, int *mode);
+/* Applies FFTB_AUTOTUNE_TILES_SCALE / _CTAS_PER_SM of a config; *mode = FFTB_AUTOTUNE_BATCH_MODE. */
+int fftb_batch_apply_config(fftb_batch batch, const char *text, int *mode);
 
 /* ------------------------------------------------------------------ allocation-free entry point */
 /* Bytes of the spectrum scratch that fftb_poisson3d_f32_noalloc keeps in static

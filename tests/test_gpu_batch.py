@@ -96,11 +96,3 @@ def test_batch_full_workload_512(B, torch_cuda):
     assert b.status(B.ROUNDTRIP) == 0
     assert float(torch.linalg.norm(out - x) / torch.linalg.norm(x)) <= TOL
 
-
-def test_partition_lpt_balances():
-    import fftm_b200.batch as B
-    shapes = B.draw_shapes(512, seed=2)
-    parts = B.partition_lpt(shapes, 4)
-    assert sorted(i for p in parts for i in p) == list(range(512))
-    loads = [sum(B.transform_bytes(shapes[i]) for i in p) for p in parts]
-    assert max(loads) / min(loads) < 1.01
