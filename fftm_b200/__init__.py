@@ -350,7 +350,7 @@ class ffts:
 
     # ------------------------------------------------------------------ strategy / autotune
     def set_strategy(self, strategy="auto", plane_cluster=0):
-        """"auto", "fused" (multi-axis kernels; plane_cluster 1, 2 or 4 CTAs per 3D
+        """"auto", "fused" (multi-axis kernels; plane_cluster 1, 2, 4 or 8 CTAs per 3D
         plane, 0 by occupancy) or "staged" (one pass kernel per axis)."""
         self._ensure()
         code = {"auto": 0, "fused": 1, "staged": 2}[strategy]

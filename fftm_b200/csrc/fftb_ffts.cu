@@ -644,7 +644,7 @@ int fftb_ffts_set_strategy(fftb_ffts o, int strategy, int plane_cluster)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
     if (strategy < FFTB_STRATEGY_AUTO || strategy > FFTB_STRATEGY_STAGED) return FFTB_ERROR_INVALID_VALUE;
-    if (plane_cluster != 0 && plane_cluster != 1 && plane_cluster != 2 && plane_cluster != 4)
+    if (plane_cluster != 0 && plane_cluster != 1 && plane_cluster != 2 && plane_cluster != 4 && plane_cluster != 8)
         return FFTB_ERROR_INVALID_VALUE;
     if (o->dim == 2) {
         if (strategy == FFTB_STRATEGY_FUSED) {

@@ -46,6 +46,9 @@ namespace fftb {
 // ever reads another CTA's shared memory.
 template <int NY, int NZ, int CL> struct PlaneShape {
     static constexpr int NT = 256;                           // threads per CTA
+    // 8-CTA clusters keep a CTA's shared memory under a third of the SM's, so three
+    // CTAs (24 warps) fit per SM when their registers are capped to match
+    static constexpr int MINB = CL >= 8 ? 3 : 1;
     static constexpr int M = NY / CL;                        // rows per CTA (z stage)
     static constexpr int S = NZ / (2 * CL);                  // column slots per CTA (y stage)
     static constexpr int NS = NZ / 2;                        // slots of the plane
@@ -78,7 +81,7 @@ template <int NY, int NZ, int CL> struct PlaneShape {
 };
 
 template <typename R, int NY, int NZ, int CL>
-__global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT)
+__global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ, CL>::MINB)
     plane_fwd_kernel(const R *__restrict__ in, cpx<R> *__restrict__ out, const cpx<R> *__restrict__ roots)
 {
     using C = cpx<R>;
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT)
 }
 
 template <typename R, int NY, int NZ, int CL>
-__global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT)
+__global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ, CL>::MINB)
     plane_inv_kernel(const cpx<R> *__restrict__ in, R *__restrict__ out, const cpx<R> *__restrict__ roots, R scale)
 {
     using C = cpx<R>;
@@ -516,10 +519,11 @@ template <typename R, int NY, int NZ, int CL> PlaneEntry plane_entry(int dtype)
 
 #define FFTB_PLANE3(R, D, NY, NZ)                                                                                   \
     plane_entry<R, NY, NZ, 1>(D), plane_entry<R, NY, NZ, 2>(D), plane_entry<R, NY, NZ, 4>(D)
+#define FFTB_PLANE4(R, D, NY, NZ) FFTB_PLANE3(R, D, NY, NZ), plane_entry<R, NY, NZ, 8>(D)
 #define FFTB_PLANES(R, D)                                                                                          \
     FFTB_PLANE3(R, D, 64, 64), FFTB_PLANE3(R, D, 64, 128), FFTB_PLANE3(R, D, 64, 256), FFTB_PLANE3(R, D, 128, 64), \
-        FFTB_PLANE3(R, D, 128, 128), FFTB_PLANE3(R, D, 128, 256), FFTB_PLANE3(R, D, 256, 64),                     \
-        FFTB_PLANE3(R, D, 256, 128), FFTB_PLANE3(R, D, 256, 256)
+        FFTB_PLANE4(R, D, 128, 128), FFTB_PLANE4(R, D, 128, 256), FFTB_PLANE3(R, D, 256, 64),                     \
+        FFTB_PLANE4(R, D, 256, 128), FFTB_PLANE4(R, D, 256, 256)
 
 const PlaneEntry *find_plane(int dtype, int ny, int nz, int cl)
 {
@@ -669,7 +673,7 @@ int fused3d_clusters(int dtype, long long nx, long long ny, long long nz, int *c
 {
     int n = 0;
     if (dtype != FFTB_F32 || !find_xcol(dtype, (int)nx)) return 0;
-    for (int cl = 1; cl <= 4; cl *= 2) {
+    for (int cl = 1; cl <= 8; cl *= 2) {
         const PlaneEntry *e = find_plane(dtype, (int)ny, (int)nz, cl);
         if (e && e->smem_fwd <= 227 * 1024 && e->smem_inv <= 227 * 1024 && n < cap) clusters[n++] = cl;
     }
@@ -686,24 +690,15 @@ int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz
     f.cluster = 0;
     if (dtype != FFTB_F32) return FFTB_SUCCESS;
     if (getenv("FFTB_DISABLE_FUSED3D")) return FFTB_SUCCESS;
+    // the smallest cluster whose plane fits the shared memory of its CTAs: measured on B200,
+    // fewer CTAs per plane wins over more resident warps (64^3, 128^3 and 256x128x256 run
+    // fastest with one CTA per plane, 256^3 with two), because every extra CTA moves a
+    // larger share of the plane through distributed shared memory and cluster barriers
     const PlaneEntry *pe = nullptr;
-    if (force_cluster > 0) {
-        const PlaneEntry *e = find_plane(dtype, (int)ny, (int)nz, force_cluster);
-        if (e && e->smem_fwd <= 227 * 1024 && e->smem_inv <= 227 * 1024) pe = e;
-    }
-    // the smallest cluster whose CTAs fit two per SM and whose grid fills two waves;
-    // failing that, the smallest one that fits one per SM
-    for (int cl = 1; cl <= 4 && !pe && force_cluster <= 0; cl *= 2) {
-        const PlaneEntry *e = find_plane(dtype, (int)ny, (int)nz, cl);
-        if (e && e->smem_fwd <= 113 * 1024 && e->smem_inv <= 113 * 1024 && nx * cl >= 2 * 148) pe = e;
-    }
-    for (int cl = 4; cl >= 1 && !pe; cl /= 2) {
-        const PlaneEntry *e = find_plane(dtype, (int)ny, (int)nz, cl);
-        if (e && e->smem_fwd <= 113 * 1024 && e->smem_inv <= 113 * 1024) pe = e;
-    }
-    for (int cl = 1; cl <= 4 && !pe; cl *= 2) {
+    for (int cl = force_cluster > 0 ? force_cluster : 1; cl <= 8 && !pe; cl *= 2) {
         const PlaneEntry *e = find_plane(dtype, (int)ny, (int)nz, cl);
         if (e && e->smem_fwd <= 227 * 1024 && e->smem_inv <= 227 * 1024) pe = e;
+        if (force_cluster > 0) break;
     }
     const XColEntry *xe = find_xcol(dtype, (int)nx);
     if (!pe || !xe) return FFTB_SUCCESS;

@@ -20,7 +20,7 @@ struct Fused3D {
 };
 
 // Sets f.enabled when (dtype, nx, ny, nz) has a specialised path.  force_cluster = 0
-// picks the plane cluster size by occupancy; 1, 2 or 4 asks for that size (f stays
+// picks the plane cluster size by occupancy; 1, 2, 4 or 8 asks for that size (f stays
 // disabled when the size has no such plane kernel).
 int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz, int force_cluster = 0);
 // The cluster sizes with plane kernels for (dtype, ny, nz) that fit the shared memory of a CTA.

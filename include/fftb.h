@@ -176,7 +176,7 @@ int fftb_ffts_timing_read(fftb_ffts obj, float *ms, double *bytes, char *names, 
  *  AUTO    the default: fused multi-axis kernels where the size has them, with the plane
  *          cluster size picked by occupancy; per-axis pass programs otherwise
  *  FUSED   fused kernels (FFTB_ERROR_UNSUPPORTED_SIZE when the size has none); for 3D,
- *          plane_cluster 1, 2 or 4 picks the CTAs per (y, z) plane (0: by occupancy)
+ *          plane_cluster 1, 2, 4 or 8 picks the CTAs per (y, z) plane (0: by occupancy)
  *  STAGED  one pass kernel per axis (the generic pass programs) */
 #define FFTB_STRATEGY_AUTO 0
 #define FFTB_STRATEGY_FUSED 1

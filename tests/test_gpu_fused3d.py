@@ -1,5 +1,5 @@
-"""GPU parity of the specialised fused 3D path (plane kernels with and without a
-2-CTA cluster, x column kernels) against the FP64 oracle, f32 tolerance 2e-6."""
+"""GPU parity of the specialised fused 3D path (plane kernels with clusters of 1, 2,
+4 and 8 CTAs per plane, x column kernels) against the FP64 oracle, f32 tolerance 2e-6."""
 import numpy as np
 import pytest
 
@@ -8,16 +8,21 @@ import oracle as O
 pytestmark = pytest.mark.gpu
 TOL = 2e-6
 
-# (nx, ny, nz): sizes with a specialised path; the comment names the plane variant chosen
+# (nx, ny, nz): sizes with a specialised path (the default picks the smallest plane
+# cluster that fits: one CTA per plane, two for 256 x 256 planes)
 FUSED = [
-    (64, 64, 64),      # 2-CTA cluster (nx < 148)
-    (256, 64, 64),     # one CTA per plane
-    (32, 128, 256),    # cluster, nx = 32
-    (64, 256, 128),    # cluster
-    (128, 128, 128),   # cluster
-    (256, 128, 64),    # one CTA per plane
-    (256, 256, 256),   # cluster, the benchmark size
+    (64, 64, 64),
+    (256, 64, 64),
+    (32, 128, 256),    # nx = 32
+    (64, 256, 128),
+    (128, 128, 128),
+    (256, 128, 64),
+    (256, 256, 256),   # 2-CTA clusters, the benchmark size
 ]
+# every plane cluster size, forced
+CLUSTERS = [((64, 64, 64), 1), ((64, 64, 64), 2), ((64, 64, 64), 4), ((32, 128, 256), 1), ((32, 128, 256), 2),
+            ((32, 128, 256), 4), ((32, 128, 256), 8), ((32, 256, 256), 2), ((32, 256, 256), 4),
+            ((32, 256, 256), 8), ((32, 256, 128), 8), ((32, 128, 128), 8)]
 
 
 @pytest.fixture(scope="module")
@@ -55,6 +60,24 @@ def test_fused_forward_backward(F, torch_cuda, shape):
     spec2 = torch.tensor(ref, dtype=torch.complex64, device="cuda")
     f.backward(spec2, out, normalized=True)
     assert O.rel_l2(_host(out), x) <= TOL
+
+
+@pytest.mark.parametrize("shape,cl", CLUSTERS)
+def test_every_plane_cluster(F, torch_cuda, shape, cl):
+    torch = torch_cuda
+    f = F.ffts("float32").init(*shape)
+    f.set_strategy("fused", cl)
+    assert f.strategy() == ("fused", cl)
+    x = O.random_3d(*shape, 77 + cl, single=True)
+    spec = torch.empty(f.spectrum_shape(), dtype=torch.complex64, device="cuda")
+    f.forward(_dev(torch, x), spec)
+    ref = O.ffts3d_forward(x)
+    assert O.rel_l2(_host(spec), ref) <= TOL
+    out = torch.empty(shape, dtype=torch.float32, device="cuda")
+    f.backward(torch.tensor(ref, dtype=torch.complex64, device="cuda"), out, normalized=True)
+    assert O.rel_l2(_host(out), x) <= TOL
+    f.poisson(_dev(torch, x), out, -1.0)
+    assert O.rel_l2(_host(out), O.poisson3d_solve(x, -1.0)) <= TOL
 
 
 @pytest.mark.parametrize("shape", FUSED)
