@@ -243,6 +243,11 @@ def main():
     ff = F.ffts("float32").init(NX, NY, NZ)
     work = torch.empty(ff.work_size // 8 + 1, dtype=torch.complex64, device=dev)
     ff.set_work_area(work)
+    # execution strategy from the project autotuner (fresh cache per run: a measured sweep of
+    # the fused plane-cluster sizes and the staged passes, least median of forward+backward)
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        tuned = ff.autotune(os.path.join(td, "fftm_autotune_3d.env"))
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.float32, device=dev)   # 1 GiB > L2
     stream = torch.cuda.current_stream()
 
@@ -474,6 +479,8 @@ def main():
         "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": DATA,
         "config": {"workload": WORKLOAD, "n": [NX, NY, NZ], "bytes_per_step": BYTES_RT,
+                   "strategy": tuned.config.get("FFTM_AUTOTUNE_STRATEGY_3D"),
+                   "autotune_median_ms": tuned.medians_ms(),
                    "l2": "flushed between steps (1 GiB write outside the timed window)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "gpu_launches": launches_per_step * args.steps,

@@ -58,6 +58,12 @@ template <int BYTES> __device__ __forceinline__ void cp_async(void *sdst, const 
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// waits until at most N of this thread's committed cp.async groups are pending
+template <int N> __device__ __forceinline__ void cp_async_wait_group()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 // Shared-memory index padding: one spare slot per 16 entries keeps the
 // stride-R Stockham scatters free of bank conflicts.

@@ -44,11 +44,9 @@ namespace fftb {
 // kz = 0 and NZ/2 results).  Data that changes owner
 // between the stages is pushed with distributed-shared-memory stores, so no CTA
 // ever reads another CTA's shared memory.
-template <int NY, int NZ, int CL> struct PlaneShape {
-    static constexpr int NT = 256;                           // threads per CTA
-    // 8-CTA clusters keep a CTA's shared memory under a third of the SM's, so three
-    // CTAs (24 warps) fit per SM when their registers are capped to match
-    static constexpr int MINB = CL >= 8 ? 3 : 1;
+template <int NY, int NZ, int CL, int NT_> struct PlaneShapeT {
+    static constexpr int NT = NT_;                           // threads per CTA
+
     static constexpr int M = NY / CL;                        // rows per CTA (z stage)
     static constexpr int S = NZ / (2 * CL);                  // column slots per CTA (y stage)
     static constexpr int NS = NZ / 2;                        // slots of the plane
@@ -78,10 +76,29 @@ template <int NY, int NZ, int CL> struct PlaneShape {
     {
         return sizeof(cpx<R>) * ((size_t)M * PR + STG + TWS);
     }
+    // CTAs per SM the register budget is sized for: 8-CTA clusters keep a CTA's shared
+    // memory under a third of the SM's, so three CTAs (24 warps) fit when registers are
+    // capped to match; smaller planes get up to 16 warps per SM as their shared memory allows
+    static constexpr int minb(size_t smem)
+    {
+        return CL >= 8 ? 3 : ((512 / NT) * smem <= 227 * 1024 ? 512 / NT : (2 * smem <= 227 * 1024 ? 2 : 1));
+    }
+    static constexpr int MINB_FWD = minb(smem_fwd<float>());
+    static constexpr int MINB_INV = minb(smem_inv<float>());
 };
 
+// Threads per CTA: 256, or fewer where the plane has fewer row pairs (z stage) or
+// column slots (y stage) than 256 threads have FFT groups, so no group idles
+template <int NY, int NZ, int CL> constexpr int plane_threads()
+{
+    constexpr int tz = RegFFTShape<NZ>::T * (NY / CL / 2), ty = RegFFTShape<NY>::T * (NZ / (2 * CL));
+    constexpr int t = tz < ty ? tz : ty;
+    return t < 256 ? (t < 32 ? 32 : t) : 256;
+}
+template <int NY, int NZ, int CL> using PlaneShape = PlaneShapeT<NY, NZ, CL, plane_threads<NY, NZ, CL>()>;
+
 template <typename R, int NY, int NZ, int CL>
-__global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ, CL>::MINB)
+__global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ, CL>::MINB_FWD)
     plane_fwd_kernel(const R *__restrict__ in, cpx<R> *__restrict__ out, const cpx<R> *__restrict__ roots)
 {
     using C = cpx<R>;
@@ -111,18 +128,35 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
         const int f = tid / TZ, t = tid - (tid / TZ) * TZ;
         C *reg = scr + f * RegFFTShape<NZ>::REGION;
         const R *rows = in + ((size_t)x * NY + (size_t)c * S::M) * NZ;
+        // the rows of the next round are loaded into registers before this round's FFT,
+        // so their memory latency overlaps the arithmetic (not with the register-capped
+        // 8-CTA clusters)
+        constexpr bool PREFETCH = CL < 8;
+        auto load_rows = [&](int p0, C (&w)[16]) {
+            const int p = p0 + f;
+            const int pp = p < S::M / 2 ? p : 0;
+            const R *ra = rows + (size_t)(2 * pp) * NZ;
+            const R *rb = ra + NZ;
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                w[r].x = ra[t + TZ * r];
+                w[r].y = rb[t + TZ * r];
+            }
+        };
+        C nxt[16];
+        if (PREFETCH) load_rows(0, nxt);
 #pragma unroll 1
         for (int p0 = 0; p0 < S::M / 2; p0 += FZ) {
             const int p = p0 + f;
             const bool ok = p < S::M / 2;
             const int pp = ok ? p : 0;
-            const R *ra = rows + (size_t)(2 * pp) * NZ;
-            const R *rb = ra + NZ;
             C v[16];
+            if (PREFETCH) {
 #pragma unroll
-            for (int r = 0; r < 16; ++r) {
-                v[r].x = ra[t + TZ * r];
-                v[r].y = rb[t + TZ * r];
+                for (int r = 0; r < 16; ++r) v[r] = nxt[r];
+                if (p0 + FZ < S::M / 2) load_rows(p0 + FZ, nxt);
+            } else {
+                load_rows(p0, v);
             }
             regfft_warp<R, NZ, -1>(v, reg, twz, t);
             // separate the two real rows with Z[-k] fetched from the partner lane:
@@ -201,29 +235,29 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
 #pragma unroll
                 for (int j = 0; j < 16; ++j) plane[(t + TY * j) * S::PF + slc] = v[j];
             }
-        }
-    }
-    __syncthreads();
-    // ---- coalesced row stores of the owned slots: out[x][ky][c*S + s]
-    {
-        C *oplane = out + (size_t)x * NY * (NZ / 2 + 1) + c * S::S;
+            // coalesced row-segment stores of this round's slots, out[x][ky][c*S + s]; they
+            // drain while the next round computes
+            __syncthreads();
+            const int ns = (S::S - s0) < FY ? (S::S - s0) : FY;
+            C *orow = oplane + c * S::S + s0;
 #pragma unroll 4
-        for (int e = tid; e < NY * S::S; e += S::NT) {
-            const int row = e / S::S, sl = e - (e / S::S) * S::S;
-            oplane[(size_t)row * (NZ / 2 + 1) + sl] = plane[row * S::PF + sl];
+            for (int e = tid; e < NY * ns; e += S::NT) {
+                const int row = e / ns, q = e - (e / ns) * ns;
+                orow[(size_t)row * (NZ / 2 + 1) + q] = plane[row * S::PF + s0 + q];
+            }
         }
     }
 }
 
 template <typename R, int NY, int NZ, int CL>
-__global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ, CL>::MINB)
+__global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ, CL>::MINB_INV)
     plane_inv_kernel(const cpx<R> *__restrict__ in, R *__restrict__ out, const cpx<R> *__restrict__ roots, R scale)
 {
     using C = cpx<R>;
     using S = PlaneShape<NY, NZ, CL>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *rowsm = reinterpret_cast<C *>(smem_raw);   // [M][PR]: this CTA's rows, every slot
-    C *stg = rowsm + S::M * S::PR;                // FFT exchange regions
+    C *stg = rowsm + S::M * S::PR;                // column staging / FFT exchange regions
     C *twz = stg + S::STG;
     C *twy = twz + NZ;
     const int tid = threadIdx.x;
@@ -245,20 +279,26 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
     {
         constexpr int TY = S::TY, FY = S::FY;
         const int f = tid / TY, t = tid - (tid / TY) * TY;
+        // stage the ns columns of block s0 (all NY rows) with coalesced asynchronous copies
+        auto stage = [&](int s0, C *buf) {
+            const int ns = (S::S - s0) < FY ? (S::S - s0) : FY;
+            for (int e = tid; e < NY * ns; e += S::NT) {
+                const int row = e / ns, sl = e - (e / ns) * ns;
+                cp_async<sizeof(C)>(&buf[sl * S::PC + row],
+                                    iplane + (size_t)row * (NZ / 2 + 1) + c * S::S + s0 + sl, true);
+            }
+            cp_async_commit();
+        };
+        stage(0, stg);
 #pragma unroll 1
         for (int s0 = 0; s0 < S::S; s0 += FY) {
             const int ns = (S::S - s0) < FY ? (S::S - s0) : FY;
-            // stage ns columns (all NY rows) with coalesced asynchronous copies
-            for (int e = tid; e < NY * ns; e += S::NT) {
-                const int row = e / ns, sl = e - (e / ns) * ns;
-                cp_async<sizeof(C)>(&stg[sl * S::PC + row],
-                                    iplane + (size_t)row * (NZ / 2 + 1) + c * S::S + s0 + sl, true);
-            }
-            cp_async_wait_all();
+            C *cur = stg;
+            cp_async_wait_group<0>();
             __syncthreads();
             const int sl = s0 + f;
             const bool ok = f < ns;
-            C *col = stg + f * S::PC;  // every group owns a column slot (idle ones compute on stale data)
+            C *col = cur + f * S::PC;  // every group owns a column slot (idle ones compute on stale data)
             C v[16];
 #pragma unroll
             for (int r = 0; r < 16; ++r) v[r] = col[t + TY * r];
@@ -287,9 +327,10 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
             for (int e = tid; e < NY * ns; e += S::NT) {
                 const int m = e / ns, q = e - (e / ns) * ns;
                 const int owner = m / S::M;
-                dst[owner][(m - owner * S::M) * S::PR + c * S::S + s0 + q] = stg[q * S::PC + m];
+                dst[owner][(m - owner * S::M) * S::PR + c * S::S + s0 + q] = cur[q * S::PC + m];
             }
-            __syncthreads();  // the staging area is reused by the next round
+            __syncthreads();  // the staging area is refilled for the next block
+            if (s0 + FY < S::S) stage(s0 + FY, stg);
         }
     }
     if constexpr (CL > 1) cg::this_cluster().sync();
