@@ -238,7 +238,8 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
             // coalesced row-segment stores of this round's slots, out[x][ky][c*S + s]; they
             // drain while the next round computes
             __syncthreads();
-            const int ns = (S::S - s0) < FY ? (S::S - s0) : FY;
+            // block width: a compile-time constant when the slots split into whole blocks
+            const int ns = S::S % FY == 0 ? FY : ((S::S - s0) < FY ? (S::S - s0) : FY);
             C *orow = oplane + c * S::S + s0;
 #pragma unroll 4
             for (int e = tid; e < NY * ns; e += S::NT) {
@@ -281,7 +282,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
         const int f = tid / TY, t = tid - (tid / TY) * TY;
         // stage the ns columns of block s0 (all NY rows) with coalesced asynchronous copies
         auto stage = [&](int s0, C *buf) {
-            const int ns = (S::S - s0) < FY ? (S::S - s0) : FY;
+            const int ns = S::S % FY == 0 ? FY : ((S::S - s0) < FY ? (S::S - s0) : FY);
             for (int e = tid; e < NY * ns; e += S::NT) {
                 const int row = e / ns, sl = e - (e / ns) * ns;
                 cp_async<sizeof(C)>(&buf[sl * S::PC + row],
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
         stage(0, stg);
 #pragma unroll 1
         for (int s0 = 0; s0 < S::S; s0 += FY) {
-            const int ns = (S::S - s0) < FY ? (S::S - s0) : FY;
+            const int ns = S::S % FY == 0 ? FY : ((S::S - s0) < FY ? (S::S - s0) : FY);
             C *cur = stg;
             cp_async_wait_group<0>();
             __syncthreads();
@@ -350,21 +351,26 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
             const C *ha_row = rowsm + (2 * pp) * S::PR;
             const C *hb_row = ha_row + S::PR;
             C v[16];
+            // n = t + TZ r with t < TZ and NZ = 16 TZ: registers r < 8 hold n < NZ/2 (k = n),
+            // r > 8 hold n > NZ/2 (k = NZ - n, conjugated); only lane t = 0 of registers 0 and 8
+            // meets the real kz = 0 / NZ/2 pair packed in slot 0
 #pragma unroll
             for (int r = 0; r < 16; ++r) {
-                const int n = t + TZ * r;
-                const bool hi = n > NZ / 2;
-                const int k = hi ? NZ - n : n;
                 C ha, hb;
-                if (k == 0 || k == NZ / 2) {
-                    // slot 0 holds kz = 0 in .x and kz = NZ/2 in .y (both real)
-                    const C pa = ha_row[0], pb = hb_row[0];
-                    ha = mk<R>(k == 0 ? pa.x : pa.y, R(0));
-                    hb = mk<R>(k == 0 ? pb.x : pb.y, R(0));
-                } else {
+                if (r < 8) {
+                    const int k = t + TZ * r;
                     ha = ha_row[k];
                     hb = hb_row[k];
-                    if (hi) { ha = cconj(ha); hb = cconj(hb); }
+                } else {
+                    const int k = TZ * (16 - r) - t;
+                    ha = cconj(ha_row[k]);
+                    hb = cconj(hb_row[k]);
+                }
+                if ((r == 0 || r == 8) && t == 0) {
+                    // slot 0 holds kz = 0 in .x and kz = NZ/2 in .y (both real)
+                    const C pa = ha_row[0], pb = hb_row[0];
+                    ha = mk<R>(r == 0 ? pa.x : pa.y, R(0));
+                    hb = mk<R>(r == 0 ? pb.x : pb.y, R(0));
                 }
                 v[r] = mk<R>(ha.x - hb.y, ha.y + hb.x);  // Ha + i Hb
             }
