@@ -39,6 +39,7 @@ NX = NY = NZ = 256
 N_REAL = NX * NY * NZ
 N_CPLX = NX * NY * (NZ // 2 + 1)
 BYTES_RT = 2 * (4 * N_REAL + 8 * N_CPLX)   # 269,484,032
+FLOPS_RT = 2 * 5 * N_REAL * 24              # 5 N log2 N per transform, two transforms
 WORKLOAD = "3D periodic Poisson solve 256^3 f32: R2C, x(-1/|k|^2) (k=0 -> 0), C2R, 1/N"
 DATA = ("synthetic: f = sin x sin 2y cos 3z + 0.1*U[-1,1] (numpy default_rng(0)), mean removed, "
         "grid x_i = 2 pi i / 256")
@@ -380,6 +381,84 @@ def main():
     except Exception as exc:  # noqa: BLE001
         sec = {"unavailable": str(exc)[:200]}
 
+    def time_events(fn, n, flush_between=True):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+        for a, b in evs:
+            if flush_between:
+                flush.zero_()
+            a.record(stream)
+            fn()
+            b.record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    # plain 256^3 round trip (forward, then normalised backward), U[-1,1] from default_rng(0)
+    more = {}
+    try:
+        xr = torch.from_numpy(np.random.default_rng(0).uniform(-1, 1, (NX, NY, NZ)).astype(np.float32)).to(dev)
+        yr = torch.empty_like(xr)
+        sr = torch.empty(ff.spectrum_shape(), dtype=torch.complex64, device=dev)
+        ms = time_events(lambda: (ff.forward(xr, sr), ff.backward(sr, yr, normalized=True)), 50)
+        t = statistics.median(ms)
+        more["roundtrip_256"] = {"workload": "3D 256^3 f32 R2C + normalised C2R, U[-1,1] default_rng(0)",
+                                 "median_us": t * 1e3, "value": BYTES_RT / (t * 1e-3) / 1e9, "unit": "GB/s",
+                                 "gflops": FLOPS_RT / (t * 1e-3) / 1e9,
+                                 "round_trip_rel_l2": float(torch.linalg.norm(yr - xr) / torch.linalg.norm(xr))}
+        del xr, yr, sr
+    except Exception as exc:  # noqa: BLE001
+        more["roundtrip_256"] = {"unavailable": str(exc)[:200]}
+    # 64^3 round trip: fits in L2, latency bound, timed as CUDA-graph replays
+    try:
+        f64 = F.ffts("float32").init(64, 64, 64)
+        w64 = torch.empty(max(1, f64.work_size // 8 + 1), dtype=torch.complex64, device=dev)
+        f64.set_work_area(w64)
+        x64 = torch.from_numpy(np.random.default_rng(0).uniform(-1, 1, (64, 64, 64)).astype(np.float32)).to(dev)
+        y64 = torch.empty_like(x64)
+        s64 = torch.empty(f64.spectrum_shape(), dtype=torch.complex64, device=dev)
+        for _ in range(3):
+            f64.forward(x64, s64)
+            f64.backward(s64, y64, normalized=True)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            f64.forward(x64, s64)
+            f64.backward(s64, y64, normalized=True)
+        g.replay()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(200):
+            g.replay()
+        b.record(stream)
+        torch.cuda.synchronize()
+        t = a.elapsed_time(b) / 200
+        b64 = 2 * (4 * 64 ** 3 + 8 * 64 * 64 * 33)
+        more["roundtrip_64_graph"] = {"workload": "3D 64^3 f32 R2C + normalised C2R, CUDA-graph replay (L2 resident)",
+                                      "us_per_round_trip": t * 1e3, "value": b64 / (t * 1e-3) / 1e9, "unit": "GB/s",
+                                      "round_trip_rel_l2": float(torch.linalg.norm(y64 - x64) / torch.linalg.norm(x64))}
+        del g
+    except Exception as exc:  # noqa: BLE001
+        more["roundtrip_64_graph"] = {"unavailable": str(exc)[:200]}
+    # 4D 64^4 native_xzwy Poisson solve
+    try:
+        f4p = F.ffts("float32", strategy_4d="native_xzwy").init(64, 64, 64, 64)
+        w4p = torch.empty(f4p.work_size // 8 + 1, dtype=torch.complex64, device=dev)
+        f4p.set_work_area(w4p)
+        x4p = torch.from_numpy(np.random.default_rng(1).standard_normal((64,) * 4).astype(np.float32)).to(dev)
+        y4p = torch.empty_like(x4p)
+        ms = time_events(lambda: f4p.poisson(x4p, y4p, -1.0), 30)
+        t = statistics.median(ms)
+        b4 = 2 * (4 * 64 ** 4 + 8 * 64 ** 3 * 33)
+        more["poisson4d_64"] = {"workload": "4D 64^4 f32 native_xzwy Poisson solve, N(0,1) default_rng(1)",
+                                "median_us": t * 1e3, "value": b4 / (t * 1e-3) / 1e9, "unit": "GB/s",
+                                "launches": f4p.num_launches("poisson")}
+        del x4p, y4p, w4p
+    except Exception as exc:  # noqa: BLE001
+        more["poisson4d_64"] = {"unavailable": str(exc)[:200]}
+
     # batched uneven 3D transforms: 512 shapes with every axis drawn from {32, 48, 64, 96, 128}
     # (numpy default_rng(2)); one step = the R2C + normalised C2R round trip of every transform.
     # The execution knobs come from the autotuner (fresh cache per run); sequential plain launches
@@ -477,6 +556,10 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "step_stats_us": {"mean": statistics.mean(step_ms) * 1e3, "median": statistics.median(step_ms) * 1e3,
+                          "stdev": (statistics.stdev(step_ms) if len(step_ms) > 1 else 0.0) * 1e3,
+                          "min": min(step_ms) * 1e3},
+        "gflops": FLOPS_RT / (total_ms / args.steps * 1e-3) / 1e9,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": DATA,
         "config": {"workload": WORKLOAD, "n": [NX, NY, NZ], "bytes_per_step": BYTES_RT,
                    "strategy": tuned.config.get("FFTM_AUTOTUNE_STRATEGY_3D"),
@@ -494,6 +577,7 @@ def main():
         "cufft_same_gpu": cufft,
         "secondary": sec,
         "batched": bat,
+        "more": more,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, secs, threads, ref = cpu_oracle_rate(f_host, 1)
