@@ -351,9 +351,10 @@ class ffts:
     # ------------------------------------------------------------------ strategy / autotune
     def set_strategy(self, strategy="auto", plane_cluster=0):
         """"auto", "fused" (multi-axis kernels; plane_cluster 1, 2, 4 or 8 CTAs per 3D
-        plane, 0 by occupancy) or "staged" (one pass kernel per axis)."""
+        plane, 0 by occupancy), "fused_tc" (fused, with the column kernels' first radix-16
+        stage on the tensor cores in split FP16) or "staged" (one pass kernel per axis)."""
         self._ensure()
-        code = {"auto": 0, "fused": 1, "staged": 2}[strategy]
+        code = {"auto": 0, "fused": 1, "staged": 2, "fused_tc": 3}[strategy]
         _check(_lib.load().fftb_ffts_set_strategy(self._h, code, int(plane_cluster)), "set_strategy")
 
     def strategy(self):
@@ -361,7 +362,7 @@ class ffts:
         self._ensure()
         s, c = ctypes.c_int(), ctypes.c_int()
         _check(_lib.load().fftb_ffts_get_strategy(self._h, ctypes.byref(s), ctypes.byref(c)), "get_strategy")
-        return ("fused" if s.value == 1 else "staged"), c.value
+        return {1: "fused", 2: "staged", 3: "fused_tc"}[s.value], c.value
 
     def apply_config(self, config):
         """Applies a tuned config (dict or KEY=VALUE text) to this object."""

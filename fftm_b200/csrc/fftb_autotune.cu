@@ -16,8 +16,9 @@
 //                   FNV-1a of a canonical device description, compatible and strict)
 // The pairs are timed with CUDA events on a private stream rather than wall clock.
 // The knobs measured here are the ffts execution strategy (fused multi-axis kernels with
-// 1, 2 or 4 CTAs per plane, or one pass kernel per axis) and, for batches, the execution
-// mode, tile height and persistent CTAs per SM.
+// 1, 2, 4 or 8 CTAs per plane, the same with tensor-core column kernels, or one pass
+// kernel per axis) and, for batches, the execution mode, tile height and persistent CTAs
+// per SM.
 #include <cuda_runtime.h>
 
 #include <sys/stat.h>
@@ -457,6 +458,13 @@ int measure_ffts(int dtype, long long nx, long long ny, long long nz, long long 
             c.b = cl[i];
             cands.push_back(c);
         }
+        if (n > 0) {
+            Candidate c;
+            c.name = "fused-tc";
+            c.a = FFTB_STRATEGY_FUSED_TC;
+            c.b = 0;
+            cands.push_back(c);
+        }
     } else if (dim == 4) {
         Fused4D f;
         if (fused4d_init(f, dtype, layout, nx, ny, nz, nw) == FFTB_SUCCESS && f.enabled) {
@@ -464,6 +472,9 @@ int measure_ffts(int dtype, long long nx, long long ny, long long nz, long long 
             c.name = "fused";
             c.a = FFTB_STRATEGY_FUSED;
             c.b = 0;
+            cands.push_back(c);
+            c.name = "fused-tc";
+            c.a = FFTB_STRATEGY_FUSED_TC;
             cands.push_back(c);
         }
     }
@@ -509,7 +520,8 @@ int measure_ffts(int dtype, long long nx, long long ny, long long nz, long long 
         set_last_error("no autotune candidate passed: " + cands.back().error);
         return FFTB_ERROR_TUNE_FAILED;
     }
-    out["FFTB_AUTOTUNE_STRATEGY"] = best->a == FFTB_STRATEGY_FUSED ? "fused" : "staged";
+    out["FFTB_AUTOTUNE_STRATEGY"] =
+        best->a == FFTB_STRATEGY_FUSED ? "fused" : (best->a == FFTB_STRATEGY_FUSED_TC ? "fused_tc" : "staged");
     out["FFTB_AUTOTUNE_PLANE_CLUSTER"] = std::to_string(best->b);
     out[dim == 4 ? "FFTM_AUTOTUNE_STRATEGY_4D" : "FFTM_AUTOTUNE_STRATEGY_3D"] = best->name;
     out["FFTB_AUTOTUNE_MEDIAN_MS"] = fmt(best->median_ms);
@@ -783,11 +795,14 @@ int fftb_ffts_apply_config(fftb_ffts obj, const char *text)
     if (st != FFTB_SUCCESS) return st;
     const std::string strat = get(c, "FFTB_AUTOTUNE_STRATEGY");
     int cl = 0;
-    if ((strat != "fused" && strat != "staged") || to_int(get(c, "FFTB_AUTOTUNE_PLANE_CLUSTER"), &cl) != FFTB_SUCCESS) {
+    if ((strat != "fused" && strat != "fused_tc" && strat != "staged") ||
+        to_int(get(c, "FFTB_AUTOTUNE_PLANE_CLUSTER"), &cl) != FFTB_SUCCESS) {
         set_last_error("autotune config has no valid FFTB_AUTOTUNE_STRATEGY / FFTB_AUTOTUNE_PLANE_CLUSTER");
         return FFTB_ERROR_CACHE_MISMATCH;
     }
-    return fftb_ffts_set_strategy(obj, strat == "fused" ? FFTB_STRATEGY_FUSED : FFTB_STRATEGY_STAGED, cl);
+    const int code =
+        strat == "fused" ? FFTB_STRATEGY_FUSED : (strat == "fused_tc" ? FFTB_STRATEGY_FUSED_TC : FFTB_STRATEGY_STAGED);
+    return fftb_ffts_set_strategy(obj, code, cl);
 }
 
 int fftb_autotune_batch(fftb_batch batch, int op, double sign, const char *cache_file, int flags, int warmup,

@@ -643,7 +643,9 @@ int fftb_ffts_num_launches(fftb_ffts o, int which, int *launches)
 int fftb_ffts_set_strategy(fftb_ffts o, int strategy, int plane_cluster)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
-    if (strategy < FFTB_STRATEGY_AUTO || strategy > FFTB_STRATEGY_STAGED) return FFTB_ERROR_INVALID_VALUE;
+    if (strategy < FFTB_STRATEGY_AUTO || strategy > FFTB_STRATEGY_FUSED_TC) return FFTB_ERROR_INVALID_VALUE;
+    const bool tc = strategy == FFTB_STRATEGY_FUSED_TC;
+    if (tc) strategy = FFTB_STRATEGY_FUSED;
     if (plane_cluster != 0 && plane_cluster != 1 && plane_cluster != 2 && plane_cluster != 4 && plane_cluster != 8)
         return FFTB_ERROR_INVALID_VALUE;
     if (o->dim == 2) {
@@ -663,6 +665,7 @@ int fftb_ffts_set_strategy(fftb_ffts o, int strategy, int plane_cluster)
             set_last_error("no fused 3D kernels for this size / dtype / plane cluster");
             return FFTB_ERROR_UNSUPPORTED_SIZE;
         }
+        f.tc = tc;
         o->fused = f;
     } else {
         Fused4D f;
@@ -677,6 +680,7 @@ int fftb_ffts_set_strategy(fftb_ffts o, int strategy, int plane_cluster)
             set_last_error("no fused 4D kernels for this size / dtype / layout");
             return FFTB_ERROR_UNSUPPORTED_SIZE;
         }
+        f.tc = tc;
         o->fused4 = f;
     }
     return FFTB_SUCCESS;
@@ -686,10 +690,10 @@ int fftb_ffts_get_strategy(fftb_ffts o, int *strategy, int *plane_cluster)
 {
     if (!o || !strategy || !plane_cluster) return FFTB_ERROR_INVALID_HANDLE;
     if (o->fused.enabled) {
-        *strategy = FFTB_STRATEGY_FUSED;
+        *strategy = o->fused.tc ? FFTB_STRATEGY_FUSED_TC : FFTB_STRATEGY_FUSED;
         *plane_cluster = o->fused.cluster;
     } else if (o->fused4.enabled) {
-        *strategy = FFTB_STRATEGY_FUSED;
+        *strategy = o->fused4.tc ? FFTB_STRATEGY_FUSED_TC : FFTB_STRATEGY_FUSED;
         *plane_cluster = 1;
     } else {
         *strategy = FFTB_STRATEGY_STAGED;

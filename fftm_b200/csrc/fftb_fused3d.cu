@@ -27,6 +27,7 @@
 #include "../../include/fftb.h"
 #include "fftb_fused3d.h"
 #include "fftb_regfft.cuh"
+#include "fftb_tc.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -404,6 +405,7 @@ struct XColEp {
     int hn;
     float hw_f;
     double hw;
+    int tc;  // host side: launch the tensor-core variant of the kernel
 };
 
 template <int NX> struct XColShape {
@@ -412,12 +414,15 @@ template <int NX> struct XColShape {
     static constexpr int NT = 256;
 };
 
-template <typename R, int NX, int SIGN>
-__device__ __forceinline__ void xcol_fft(cpx<R> (&v)[16], cpx<R> *scr, const cpx<R> *tw, int t, int col)
+// TC: the first radix-16 stage runs on the tensor cores (fftb_tc.cuh, float only)
+template <typename R, int NX, int SIGN, bool TC>
+__device__ __forceinline__ void xcol_fft(cpx<R> (&v)[16], cpx<R> *scr, const cpx<R> *tw, int t, int col,
+                                         unsigned char *stage, const TcDft16 &F)
 {
     using C = cpx<R>;
     constexpr int T = XColShape<NX>::T, W = XColShape<NX>::W;
-    dft16<SIGN, C, R>(v);
+    if constexpr (TC) tc_dft16<SIGN>(v, stage, F, (int)(threadIdx.x & 31));
+    else dft16<SIGN, C, R>(v);
 #pragma unroll
     for (int k1 = 1; k1 < 16; ++k1) v[k1] = twiddle_mul<SIGN>(v[k1], tw, t * k1);
     __syncthreads();
@@ -441,7 +446,7 @@ __device__ __forceinline__ void xcol_fft(cpx<R> (&v)[16], cpx<R> *scr, const cpx
 // 4: inverse of 3: reads the rows tin[col][kx], writes the columns in place of `data`.
 // blockIdx.y selects a batch of column sets `bstride` elements apart (the transposed
 // side has NX * ncols elements per batch).
-template <typename R, int NX, int MODE>
+template <typename R, int NX, int MODE, bool TC>
 __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data, long long stride, int ncols,
                                                    long long bstride, cpx<R> *__restrict__ tdata,
                                                    const cpx<R> *__restrict__ roots, XColEp ep)
@@ -452,6 +457,10 @@ __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data,
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *scr = reinterpret_cast<C *>(smem_raw);
     C *tw = scr + (16 * T * W > W * RP ? 16 * T * W : W * RP);
+    // TC: each warp's tensor-core staging area follows the twiddles
+    unsigned char *stage = reinterpret_cast<unsigned char *>(tw + NX) + (threadIdx.x >> 5) * kTcWarpBytes;
+    TcDft16 F;
+    if constexpr (TC) tc_build_dft16(F, (int)(threadIdx.x & 31));
     const int tid = threadIdx.x;
     const int t = tid / W, col = tid - (tid / W) * W;
     for (int i = tid; i < NX; i += 256) tw[i] = roots[i];
@@ -476,8 +485,8 @@ __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data,
         for (int r = 0; r < 16; ++r) v[r] = p[(size_t)(t + T * r) * stride];
     }
     __syncthreads();
-    if (MODE == 1 || MODE == 4) xcol_fft<R, NX, +1>(v, scr, tw, t, col);
-    else xcol_fft<R, NX, -1>(v, scr, tw, t, col);
+    if (MODE == 1 || MODE == 4) xcol_fft<R, NX, +1, TC>(v, scr, tw, t, col, stage, F);
+    else xcol_fft<R, NX, -1, TC>(v, scr, tw, t, col, stage, F);
     if (MODE == 2) {
         // wavenumbers: kx = t + T*j (output row); ky, kz, kw from the column
         int ky_i, kz, kw = 0;
@@ -519,7 +528,7 @@ __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data,
                 v[j] = cscale(v[j], fct);
             }
         }
-        xcol_fft<R, NX, +1>(v, scr, tw, t, col);
+        xcol_fft<R, NX, +1, TC>(v, scr, tw, t, col, stage, F);
     }
     if (MODE != 2 && (ep.mode & EP_HALFW)) {
         const int ih = cg0 % (ep.hn / 2 + 1);
@@ -584,18 +593,25 @@ struct XColEntry {
     int dtype, nx;
     const void *fn[5];
     size_t smem;
+    const void *fn_tc[5];  // first radix-16 stage on the tensor cores
+    size_t smem_tc;
 };
 
 template <typename R, int NX> XColEntry xcol_entry(int dtype)
 {
     constexpr int T = XColShape<NX>::T, W = XColShape<NX>::W;
     constexpr size_t scr = (size_t)16 * T * W > (size_t)W * (NX + 1) ? (size_t)16 * T * W : (size_t)W * (NX + 1);
+    constexpr size_t smem = sizeof(cpx<R>) * (scr + NX);
     return XColEntry{dtype,
                      NX,
-                     {(const void *)&xcol_kernel<R, NX, 0>, (const void *)&xcol_kernel<R, NX, 1>,
-                      (const void *)&xcol_kernel<R, NX, 2>, (const void *)&xcol_kernel<R, NX, 3>,
-                      (const void *)&xcol_kernel<R, NX, 4>},
-                     sizeof(cpx<R>) * (scr + NX)};
+                     {(const void *)&xcol_kernel<R, NX, 0, false>, (const void *)&xcol_kernel<R, NX, 1, false>,
+                      (const void *)&xcol_kernel<R, NX, 2, false>, (const void *)&xcol_kernel<R, NX, 3, false>,
+                      (const void *)&xcol_kernel<R, NX, 4, false>},
+                     smem,
+                     {(const void *)&xcol_kernel<R, NX, 0, true>, (const void *)&xcol_kernel<R, NX, 1, true>,
+                      (const void *)&xcol_kernel<R, NX, 2, true>, (const void *)&xcol_kernel<R, NX, 3, true>,
+                      (const void *)&xcol_kernel<R, NX, 4, true>},
+                     smem + (size_t)(256 / 32) * kTcWarpBytes};
 }
 
 const XColEntry *find_xcol(int dtype, int nx)
@@ -699,7 +715,8 @@ int launch_xcol_n(const XColEntry *e, int mode, void *data, long long stride, lo
     const float2 *rt = (const float2 *)roots;
     void *args[] = {&d, &stride, &nc, &bstride, &td, &rt, &x};
     const dim3 grid((unsigned)((ncols + W - 1) / W), (unsigned)nbatch);
-    return set_status_from_cuda(cudaLaunchKernel(e->fn[mode], grid, dim3(256), args, e->smem, s));
+    return set_status_from_cuda(cudaLaunchKernel(x.tc ? e->fn_tc[mode] : e->fn[mode], grid, dim3(256), args,
+                                                 x.tc ? e->smem_tc : e->smem, s));
 }
 
 int launch_xcol(const Fused3D &f, int mode, void *data, const EpValues *ep, cudaStream_t s, LaunchTimer *tm)
@@ -711,6 +728,7 @@ int launch_xcol(const Fused3D &f, int mode, void *data, const EpValues *ep, cuda
     x.ny = (int)f.ny;
     x.nz = (int)f.nz;
     x.hn = (int)f.nz;
+    x.tc = f.tc ? 1 : 0;
     return launch_xcol_n((const XColEntry *)f.xcol, mode, data, ncols, ncols, 1, 0, nullptr, f.roots_x, x, s, tm);
 }
 
@@ -753,7 +771,9 @@ int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz
     if ((st = configure(pe->fwd, pe->smem_fwd)) != FFTB_SUCCESS) return st;
     if ((st = configure(pe->inv, pe->smem_inv)) != FFTB_SUCCESS) return st;
     for (int m = 0; m < 5; ++m)
-        if ((st = configure(xe->fn[m], xe->smem)) != FFTB_SUCCESS) return st;
+        if ((st = configure(xe->fn[m], xe->smem)) != FFTB_SUCCESS ||
+            (st = configure(xe->fn_tc[m], xe->smem_tc)) != FFTB_SUCCESS)
+            return st;
     const int nmax = (int)(ny > nz ? ny : nz);
     if ((st = engine_roots(dtype, nmax, &f.roots_plane)) != FFTB_SUCCESS) return st;
     if ((st = engine_roots(dtype, (int)nx, &f.roots_x)) != FFTB_SUCCESS) return st;
@@ -844,7 +864,9 @@ int fused4d_init(Fused4D &f, int dtype, int layout, long long nx, long long ny, 
     if ((st = configure(pe->inv, pe->smem_inv)) != FFTB_SUCCESS) return st;
     for (const XColEntry *e : {xe, ye})
         for (int m = 0; m < 5; ++m)
-            if ((st = configure(e->fn[m], e->smem)) != FFTB_SUCCESS) return st;
+            if ((st = configure(e->fn[m], e->smem)) != FFTB_SUCCESS ||
+                (st = configure(e->fn_tc[m], e->smem_tc)) != FFTB_SUCCESS)
+                return st;
     const int nmax = (int)(nz > nw ? nz : nw);
     if ((st = engine_roots(dtype, nmax, &f.roots_plane)) != FFTB_SUCCESS) return st;
     if ((st = engine_roots(dtype, (int)nx, &f.roots_x)) != FFTB_SUCCESS) return st;
@@ -866,6 +888,7 @@ XColEp ep4(const Fused4D &f, const EpValues *ep)
     x.nwh = (int)(f.nw / 2 + 1);
     x.nzh = 1;
     x.hn = (int)f.nw;
+    x.tc = f.tc ? 1 : 0;
     return x;
 }
 } // namespace

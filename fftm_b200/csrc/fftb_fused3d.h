@@ -13,6 +13,7 @@ struct Fused3D {
     int dtype = 0;
     long long nx = 0, ny = 0, nz = 0;
     int cluster = 0;               // CTAs per (y, z) plane of the selected plane kernels
+    bool tc = false;               // column kernels with the first radix-16 stage on the tensor cores
     const void *plane = nullptr;   // selected plane kernel entry
     const void *xcol = nullptr;    // selected x column kernel entry
     void *roots_plane = nullptr;   // device root table of length max(ny, nz)
@@ -38,6 +39,7 @@ struct Fused4D {
     bool enabled = false;
     int dtype = 0, layout = 0;
     long long nx = 0, ny = 0, nz = 0, nw = 0;
+    bool tc = false;               // column kernels with the first radix-16 stage on the tensor cores
     const void *plane = nullptr, *xcol = nullptr, *ycol = nullptr;
     void *roots_plane = nullptr, *roots_x = nullptr, *roots_y = nullptr;
 };

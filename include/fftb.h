@@ -177,12 +177,16 @@ int fftb_ffts_timing_read(fftb_ffts obj, float *ms, double *bytes, char *names, 
  *          cluster size picked by occupancy; per-axis pass programs otherwise
  *  FUSED   fused kernels (FFTB_ERROR_UNSUPPORTED_SIZE when the size has none); for 3D,
  *          plane_cluster 1, 2, 4 or 8 picks the CTAs per (y, z) plane (0: by occupancy)
- *  STAGED  one pass kernel per axis (the generic pass programs) */
+ *  STAGED  one pass kernel per axis (the generic pass programs)
+ *  FUSED_TC  FUSED with the column kernels (3D: x; 4D: y and x) running their first
+ *          radix-16 stage as a 16x16 complex contraction on the tensor cores in split
+ *          FP16 (head + tail operands, FP32 accumulation); float32 only */
 #define FFTB_STRATEGY_AUTO 0
 #define FFTB_STRATEGY_FUSED 1
 #define FFTB_STRATEGY_STAGED 2
+#define FFTB_STRATEGY_FUSED_TC 3
 int fftb_ffts_set_strategy(fftb_ffts obj, int strategy, int plane_cluster);
-/* the strategy in effect (FUSED or STAGED) and its plane cluster size (0 when STAGED) */
+/* the strategy in effect (FUSED, FUSED_TC or STAGED) and its plane cluster size (0 when STAGED) */
 int fftb_ffts_get_strategy(fftb_ffts obj, int *strategy, int *plane_cluster);
 
 /* ------------------------------------------------------------------ batched uneven 3D transforms */

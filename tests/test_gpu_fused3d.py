@@ -127,3 +127,26 @@ def test_fused_round_trip_criterion_256(F, torch_cuda):
     f.backward(spec, out, normalized=True)
     rms = torch.sqrt(torch.mean((out - x) ** 2)).item()
     assert rms <= 10 * np.finfo(np.float32).eps
+
+
+TC_TOL = 5e-6
+
+
+@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 128, 256), (128, 128, 64), (256, 256, 256)])
+def test_fused_tensor_core_form(F, torch_cuda, shape):
+    """Split-FP16 tensor-core x column kernel: relative L2 vs the FP64 oracle <= 5e-6."""
+    torch = torch_cuda
+    f = F.ffts("float32").init(*shape)
+    f.set_strategy("fused_tc")
+    assert f.strategy()[0] == "fused_tc"
+    x = O.random_3d(*shape, 0x5EED, single=True)
+    spec = torch.empty(f.spectrum_shape(), dtype=torch.complex64, device="cuda")
+    f.forward(_dev(torch, x), spec)
+    err_f = O.rel_l2(_host(spec), O.ffts3d_forward(x))
+    out = torch.empty(shape, dtype=torch.float32, device="cuda")
+    f.backward(spec, out, normalized=True)
+    err_rt = O.rel_l2(_host(out), x)
+    f.poisson(_dev(torch, x), out, -1.0)
+    err_p = O.rel_l2(_host(out), O.poisson3d_solve(x, -1.0))
+    print(f"tensor-core form {shape}: forward {err_f:.2e}, round trip {err_rt:.2e}, Poisson {err_p:.2e}")
+    assert err_f <= TC_TOL and err_rt <= TC_TOL and err_p <= TC_TOL

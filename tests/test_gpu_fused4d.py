@@ -85,3 +85,26 @@ def test_fused4d_poisson_manufactured_64(F, torch_cuda):
         sol = torch.empty(dims, dtype=torch.float32, device="cuda")
         f.poisson(_dev(torch, 15 * u), sol, +1.0)
         assert O.rel_l2(_host(sol), u) <= TOL
+
+
+TC_TOL = 5e-6
+
+
+@pytest.mark.parametrize("dims", [(32, 64, 128, 64), (64, 64, 64, 64)])
+def test_fused4d_tensor_core_form(F, torch_cuda, dims):
+    """Split-FP16 tensor-core column kernels: relative L2 vs the FP64 oracle <= 5e-6."""
+    torch = torch_cuda
+    f = F.ffts("float32", strategy_4d="native_xzwy").init(*dims)
+    f.set_strategy("fused_tc")
+    assert f.strategy()[0] == "fused_tc"
+    x = O.random_4d(*dims, 1, layout=O.NATIVE_XZWY, single=True)
+    spec = torch.empty(f.spectrum_shape(), dtype=torch.complex64, device="cuda")
+    f.forward(_dev(torch, x), spec)
+    err_f = O.rel_l2(_host(spec), O.ffts4d_forward(O.NATIVE_XZWY, x, dims))
+    out = torch.empty(f.real_shape(), dtype=torch.float32, device="cuda")
+    f.backward(spec, out, normalized=True)
+    err_rt = O.rel_l2(_host(out), x)
+    f.poisson(_dev(torch, x), out, -1.0)
+    err_p = O.rel_l2(_host(out), O.poisson4d_solve(O.NATIVE_XZWY, x, dims, -1.0))
+    print(f"tensor-core form {dims}: forward {err_f:.2e}, round trip {err_rt:.2e}, Poisson {err_p:.2e}")
+    assert err_f <= TC_TOL and err_rt <= TC_TOL and err_p <= TC_TOL
