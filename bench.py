@@ -519,8 +519,10 @@ def main():
 
     # batched uneven 3D transforms: 512 shapes with every axis drawn from {32, 48, 64, 96, 128}
     # (numpy default_rng(2)); one step = the R2C + normalised C2R round trip of every transform.
-    # The execution knobs come from the autotuner (fresh cache per run); sequential plain launches
-    # of the same batch are timed beside it.  With N > 1 each rank runs its LPT share.
+    # The execution mode and knobs come from the autotuner (fresh cache per run): the grouped
+    # launches (one per stage and line length) or the single persistent launch, each replayed
+    # from a CUDA graph; the persistent launch and 2560 sequential plain launches of the same
+    # batch are timed beside it.  With N > 1 each rank runs its LPT share.
     bat = None
     try:
         import tempfile
@@ -554,9 +556,10 @@ def main():
         if dist is not None:
             dist.barrier()
         tuned_ms = replicas.max_over_ranks(dist, time_batch(bt.mode, 10), dev) / 10
-        status = bt.status(B.ROUNDTRIP)
         berr = float(torch.linalg.norm(by - bx) / torch.linalg.norm(bx))
         seq_ms = replicas.max_over_ranks(dist, time_batch(B.SEQUENTIAL, 5), dev) / 5
+        pers_ms = replicas.max_over_ranks(dist, time_batch(B.GRAPH, 10), dev) / 10
+        pers_status = bt.status(B.ROUNDTRIP)
         total_bytes = sum(B.transform_bytes(s_) for s_ in shapes)
         bat = {"workload": "512 uneven 3D f32 R2C + normalised C2R round trips, axes from {32,48,64,96,128}, "
                            "numpy default_rng(2)",
@@ -565,8 +568,12 @@ def main():
                "tuned": {k: sel.config.get(k) for k in ("FFTM_AUTOTUNE_STRATEGY_3D", "FFTB_AUTOTUNE_BATCH_MODE",
                                                        "FFTB_AUTOTUNE_TILES_SCALE", "FFTB_AUTOTUNE_CTAS_PER_SM")},
                "candidates_median_ms": sel.medians_ms(),
-               "launches_per_step": 1 if bt.mode != B.SEQUENTIAL else bt.describe(B.ROUNDTRIP)["passes"],
-               "wait_error_flag": status, "round_trip_rel_l2": berr,
+               "mode": {0: "sequential", 1: "persistent", 2: "persistent, graph", 3: "grouped",
+                        4: "grouped, graph"}[bt.mode],
+               "graph_launches_per_step": 1 if bt.mode in (B.GRAPH, B.GROUPED_GRAPH) else None,
+               "round_trip_rel_l2": berr,
+               "persistent_single_launch": {"ms_per_step": pers_ms, "value": total_bytes / (pers_ms * 1e-3) / 1e9,
+                                            "kernel_launches_per_step": 1, "wait_error_flag": pers_status},
                "sequential_plain_launches": {"ms_per_step": seq_ms,
                                              "value": total_bytes / (seq_ms * 1e-3) / 1e9,
                                              "launches_per_step": bt.describe(B.ROUNDTRIP)["passes"]}}

@@ -2,7 +2,9 @@
 
 :class:`Batch` packs many 3D transforms of different (nx, ny, nz) into flat device
 arrays and runs them either one transform after another (mode 0), in one
-persistent launch (mode 1) or in that launch replayed from a CUDA graph (mode 2).
+persistent launch (mode 1), in that launch replayed from a CUDA graph (mode 2), or as
+one plain launch per (stage, line length) group (mode 3; mode 4 replays those from a
+CUDA graph).
 
 :func:`partition_lpt` splits a batch over GPUs for the multi-GPU form: the
 transforms are independent, so each rank takes a subset (greedy longest-
@@ -18,7 +20,7 @@ import numpy as np
 from . import _check, _dtype_code, _lib, _ptr, _stream_ptr
 
 FORWARD, BACKWARD, ROUNDTRIP, POISSON = 0, 1, 2, 3
-SEQUENTIAL, PERSISTENT, GRAPH = 0, 1, 2
+SEQUENTIAL, PERSISTENT, GRAPH, GROUPED, GROUPED_GRAPH = 0, 1, 2, 3, 4
 
 
 def transform_bytes(shape, real_bytes=4) -> int:
@@ -106,8 +108,8 @@ class Batch:
         return sel
 
     def exec(self, op, inp, out, sign=-1.0, mode=None, stream=None):
-        """mode: SEQUENTIAL, PERSISTENT or GRAPH; None takes the tuned mode (GRAPH if the
-        batch was never tuned)."""
+        """mode: SEQUENTIAL, PERSISTENT, GRAPH, GROUPED or GROUPED_GRAPH; None takes the
+        tuned mode (GRAPH if the batch was never tuned)."""
         if mode is None:
             mode = self.mode
         L = _lib.load()

@@ -575,7 +575,7 @@ int measure_batch(fftb_batch b, int op, double sign, int warmup, int iters, Conf
         c.b = 1;
         cands.push_back(c);
     }
-    if (dtype == FFTB_F32)
+    if (dtype == FFTB_F32) {
         for (int ts : {1, 2})
             for (int cps : {0, 1, 2}) {
                 Candidate c;
@@ -585,6 +585,15 @@ int measure_batch(fftb_batch b, int op, double sign, int warmup, int iters, Conf
                 c.c = cps;
                 cands.push_back(c);
             }
+        for (int ts : {1, 2}) {
+            Candidate c;
+            c.name = "grouped-graph-t" + std::to_string(ts);
+            c.a = 4;
+            c.b = ts;
+            c.c = 0;
+            cands.push_back(c);
+        }
+    }
     const bool in_spec = op == FFTB_BATCH_BACKWARD, out_spec = op == FFTB_BATCH_FORWARD;
     const size_t nin = in_spec ? (size_t)stot * 2 : (size_t)rtot;     // reals
     const size_t nout = out_spec ? (size_t)stot * 2 : (size_t)rtot;
@@ -627,7 +636,7 @@ int measure_batch(fftb_batch b, int op, double sign, int warmup, int iters, Conf
             if (it >= warmup) times.push_back(ms);
         }
         int flag = 0;
-        if (st == FFTB_SUCCESS && c.a != 0) st = fftb_batch_status(b, op, &flag);
+        if (st == FFTB_SUCCESS && (c.a == 1 || c.a == 2)) st = fftb_batch_status(b, op, &flag);
         std::vector<double> got;
         if (st == FFTB_SUCCESS) st = sample(outb.p, nout, dtype, got);
         if (st != FFTB_SUCCESS) {
@@ -834,7 +843,7 @@ int fftb_batch_apply_config(fftb_batch batch, const char *text, int *mode)
     int m = 0, ts = 0, cps = 0;
     if (to_int(get(c, "FFTB_AUTOTUNE_BATCH_MODE"), &m) != FFTB_SUCCESS ||
         to_int(get(c, "FFTB_AUTOTUNE_TILES_SCALE"), &ts) != FFTB_SUCCESS ||
-        to_int(get(c, "FFTB_AUTOTUNE_CTAS_PER_SM"), &cps) != FFTB_SUCCESS || m < 0 || m > 2) {
+        to_int(get(c, "FFTB_AUTOTUNE_CTAS_PER_SM"), &cps) != FFTB_SUCCESS || m < 0 || m > 4) {
         set_last_error("autotune config has no valid FFTB_AUTOTUNE_BATCH_MODE / _TILES_SCALE / _CTAS_PER_SM");
         return FFTB_ERROR_CACHE_MISMATCH;
     }

@@ -122,6 +122,42 @@ __global__ void __launch_bounds__(kBatchThreads)
     }
 }
 
+// Grouped form: one plain launch per (stage, line length) over the tiles of every
+// transform in that group, each CTA one (pass, tile) item.  Every launch is specialised
+// for its line length, so there is no register union and no dependency wait: stream
+// order separates the stages.
+__device__ __forceinline__ const void *batch_buf(int k, const void *in, void *out, void *work)
+{
+    return k == 0 ? in : (k == 1 ? (const void *)out : (const void *)work);
+}
+
+template <int NF>
+__global__ void __launch_bounds__(kBatchThreads)
+    batch_group_kernel(const BatchItem *__restrict__ items, const PassArgs *__restrict__ passes,
+                       const PassBind *__restrict__ binds, const void *in, void *out, void *work)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const BatchItem bi = items[blockIdx.x];
+    PassArgs a = passes[bi.pass];
+    const PassBind b = binds[bi.pass];
+    a.in = (const char *)batch_buf(b.in_buf, in, out, work) + b.in_off;
+    a.out = (char *)const_cast<void *>(batch_buf(b.out_buf, in, out, work)) + b.out_off;
+    pass_body<float, NF, false>(a, (long long)bi.tile * a.G, smem_raw);
+}
+
+const void *batch_group_fn(int nf)
+{
+    switch (nf) {
+#define FFTB_CASE(n)                                                                                                  \
+    case n:                                                                                                           \
+        return (const void *)&batch_group_kernel<n>;
+        FFTB_BATCH_NF_LIST(FFTB_CASE)
+#undef FFTB_CASE
+    default:
+        return nullptr;
+    }
+}
+
 bool batch_nf_supported(int nf)
 {
     switch (nf) {
@@ -156,8 +192,17 @@ struct OpPlan {
     int *d_deps = nullptr, *d_ntiles = nullptr;
     int *d_ctl = nullptr;
     int grid = 0;
+    // grouped form: the items ordered by (stage, line length), one launch per group
+    struct Group {
+        int offset, count, nf;
+        size_t smem;
+    };
+    std::vector<Group> groups;
+    BatchItem *d_gitems = nullptr;
+    // CUDA graph of the persistent launch (mode 2) or of the grouped launches (mode 4)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
+    int g_mode = 0;
     const void *g_in = nullptr;
     void *g_out = nullptr, *g_work = nullptr;
     bool persistent_ok = false;
@@ -267,6 +312,7 @@ int build_plan(fftb_batch_s *b, int op, double sign)
     std::vector<PassBind> binds(P.npasses);
     std::vector<int> deps(P.npasses, -1), ntiles(P.npasses, 0);
     size_t smem = 0;
+    std::vector<size_t> pass_smem(P.npasses, 0);
     for (int p = 0; p < P.npasses; ++p) {
         const Launch &L = P.seq.launches[p];
         PassArgs a = L.args;
@@ -282,6 +328,7 @@ int build_plan(fftb_batch_s *b, int op, double sign)
         const size_t cb = complex_bytes(b->dtype);
         const size_t sm = (a.tw_smem ? (size_t)a.ntw * cb : 0) + (size_t)G * 32 + (size_t)G * L.k.line_pitch * cb;
         smem = std::max(smem, sm);
+        pass_smem[p] = sm;
         args[p] = a;
         binds[p] = PassBind{L.in_buf, L.out_buf, (long long)L.in_off_bytes, (long long)L.out_off_bytes, L.k.nf};
         ntiles[p] = (int)((a.nlines + G - 1) / G);
@@ -296,12 +343,33 @@ int build_plan(fftb_batch_s *b, int op, double sign)
         }
     P.nitems = (int)items.size();
     P.smem = smem;
+    // grouped order: within each stage, the items of each line length together
+    std::vector<BatchItem> gitems;
+    gitems.reserve(items.size());
+    for (int s = 0; s < P.nstages; ++s) {
+        std::vector<int> nfs;
+        for (int i = 0; i < b->count; ++i) nfs.push_back(binds[tpass[i][s]].nf);
+        std::sort(nfs.begin(), nfs.end());
+        nfs.erase(std::unique(nfs.begin(), nfs.end()), nfs.end());
+        for (int nf : nfs) {
+            OpPlan::Group g{(int)gitems.size(), 0, nf, 0};
+            for (int i = 0; i < b->count; ++i) {
+                const int p = tpass[i][s];
+                if (binds[p].nf != nf) continue;
+                g.smem = std::max(g.smem, pass_smem[p]);
+                for (int t = 0; t < ntiles[p]; ++t) gitems.push_back(BatchItem{p, t});
+            }
+            g.count = (int)gitems.size() - g.offset;
+            if (g.count > 0) P.groups.push_back(g);
+        }
+    }
     if (P.persistent_ok) {
         auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
         const size_t s_items = al(items.size() * sizeof(BatchItem)), s_args = al(args.size() * sizeof(PassArgs)),
                      s_binds = al(binds.size() * sizeof(PassBind)), s_deps = al(deps.size() * sizeof(int)),
                      s_nt = al(ntiles.size() * sizeof(int)), s_ctl = al((2 + P.npasses) * sizeof(int));
-        const size_t tot = s_items + s_args + s_binds + s_deps + s_nt + s_ctl;
+        const size_t s_gitems = al(gitems.size() * sizeof(BatchItem));
+        const size_t tot = s_items + s_args + s_binds + s_deps + s_nt + s_ctl + s_gitems;
         cudaError_t e = cudaMalloc(&P.blob, tot);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -313,13 +381,19 @@ int build_plan(fftb_batch_s *b, int op, double sign)
         P.d_binds = (PassBind *)q; q += s_binds;
         P.d_deps = (int *)q; q += s_deps;
         P.d_ntiles = (int *)q; q += s_nt;
-        P.d_ctl = (int *)q;
+        P.d_ctl = (int *)q; q += s_ctl;
+        P.d_gitems = (BatchItem *)q;
         e = cudaMemcpy(P.d_items, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(P.d_passes, args.data(), args.size() * sizeof(PassArgs), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(P.d_binds, binds.data(), binds.size() * sizeof(PassBind), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(P.d_deps, deps.data(), deps.size() * sizeof(int), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(P.d_ntiles, ntiles.data(), ntiles.size() * sizeof(int), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemset(P.d_ctl, 0, (2 + P.npasses) * sizeof(int));
+        if (e == cudaSuccess)
+            e = cudaMemcpy(P.d_gitems, gitems.data(), gitems.size() * sizeof(BatchItem), cudaMemcpyHostToDevice);
+        for (const OpPlan::Group &g : P.groups)
+            if (e == cudaSuccess && g.smem > 48 * 1024)
+                e = cudaFuncSetAttribute(batch_group_fn(g.nf), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem);
         if (e != cudaSuccess) return set_status_from_cuda(e);
         if (smem > 48 * 1024) {
             e = cudaFuncSetAttribute((const void *)batch_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -347,6 +421,20 @@ int launch_persistent(OpPlan &P, const void *in, void *out, void *work, cudaStre
     batch_persistent_kernel<<<P.grid, kBatchThreads, P.smem, s>>>(P.d_items, P.nitems, P.d_passes, P.d_binds,
                                                                  P.d_deps, P.d_ntiles, P.d_ctl, in, out, work);
     return set_status_from_cuda(cudaGetLastError());
+}
+
+int launch_groups(OpPlan &P, const void *in, void *out, void *work, cudaStream_t s)
+{
+    for (const OpPlan::Group &g : P.groups) {
+        const BatchItem *items = P.d_gitems + g.offset;
+        const PassArgs *passes = P.d_passes;
+        const PassBind *binds = P.d_binds;
+        void *args[] = {&items, &passes, &binds, &in, &out, &work};
+        cudaError_t e = cudaLaunchKernel(batch_group_fn(g.nf), dim3((unsigned)g.count), dim3(kBatchThreads), args,
+                                         g.smem, s);
+        if (e != cudaSuccess) return set_status_from_cuda(e);
+    }
+    return FFTB_SUCCESS;
 }
 
 int ensure_work(fftb_batch_s *b)
@@ -465,7 +553,7 @@ int fftb_batch_set_tuning(fftb_batch b, int tiles_scale, int ctas_per_sm)
 int fftb_batch_exec(fftb_batch b, int op, const void *in, void *out, double sign, int mode)
 {
     if (!b) return FFTB_ERROR_INVALID_HANDLE;
-    if (op < 0 || op >= OP_COUNT || !in || !out || mode < 0 || mode > 2) return FFTB_ERROR_INVALID_VALUE;
+    if (op < 0 || op >= OP_COUNT || !in || !out || mode < 0 || mode > 4) return FFTB_ERROR_INVALID_VALUE;
     int st = build_plan(b, op, sign);
     if (st != FFTB_SUCCESS) return st;
     OpPlan &P = b->ops[op];
@@ -480,8 +568,9 @@ int fftb_batch_exec(fftb_batch b, int op, const void *in, void *out, double sign
     }
     if ((uintptr_t)in % 16 || (uintptr_t)out % 16 || (uintptr_t)work % 16) return FFTB_ERROR_MISALIGNED;
     if (mode == 1) return launch_persistent(P, in, out, work, b->stream);
-    // mode 2: replay the captured graph (captured on first use of this binding)
-    if (!P.gexec || P.g_in != in || P.g_out != out || P.g_work != work) {
+    if (mode == 3) return launch_groups(P, in, out, work, b->stream);
+    // modes 2 and 4: replay the captured graph (captured on first use of this binding)
+    if (!P.gexec || P.g_mode != mode || P.g_in != in || P.g_out != out || P.g_work != work) {
         if (P.gexec) cudaGraphExecDestroy(P.gexec);
         if (P.graph) cudaGraphDestroy(P.graph);
         P.gexec = nullptr;
@@ -491,17 +580,20 @@ int fftb_batch_exec(fftb_batch b, int op, const void *in, void *out, double sign
         if (e != cudaSuccess) return set_status_from_cuda(e);
         e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            st = launch_persistent(P, in, out, work, cap);
+            st = mode == 2 ? launch_persistent(P, in, out, work, cap) : launch_groups(P, in, out, work, cap);
             cudaGraph_t g = nullptr;
             e = cudaStreamEndCapture(cap, &g);
             if (st == FFTB_SUCCESS && e == cudaSuccess) {
                 P.graph = g;
                 e = cudaGraphInstantiate(&P.gexec, g, 0);
+            } else if (g) {
+                cudaGraphDestroy(g);
             }
         }
         cudaStreamDestroy(cap);
         if (st != FFTB_SUCCESS) return st;
         if (e != cudaSuccess) return set_status_from_cuda(e);
+        P.g_mode = mode;
         P.g_in = in;
         P.g_out = out;
         P.g_work = work;

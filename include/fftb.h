@@ -197,7 +197,8 @@ int fftb_ffts_get_strategy(fftb_ffts obj, int *strategy, int *plane_cluster);
  * all transforms run either one transform after another (mode 0, plain launches) or
  * in ONE persistent launch that takes (pass, tile) items from a stage-ordered work
  * list with per-pass completion counters (mode 1), replayed from a CUDA graph captured
- * per buffer binding (mode 2).  Persistent modes are float32; float64 batches run mode 0. */
+ * per buffer binding (mode 2), or as one launch per (stage, line length) group (modes 3,
+ * 4).  Modes 1-4 are float32; float64 batches run mode 0. */
 typedef struct fftb_batch_s *fftb_batch;
 #define FFTB_BATCH_FORWARD 0   /* in: packed real, out: packed spectrum */
 #define FFTB_BATCH_BACKWARD 1  /* in: packed spectrum (overwritten), out: packed real, 1/N scaled */
@@ -215,7 +216,10 @@ int fftb_batch_set_stream(fftb_batch batch, void *stream);
  * at most ctas_per_sm persistent CTAs per SM (0: the occupancy limit). */
 int fftb_batch_set_tuning(fftb_batch batch, int tiles_scale, int ctas_per_sm);
 /* op: FFTB_BATCH_*; sign: Poisson sign (ignored otherwise); mode: 0 sequential plain
- * launches, 1 one persistent launch, 2 persistent launch replayed from a CUDA graph. */
+ * launches, 1 one persistent launch, 2 persistent launch replayed from a CUDA graph,
+ * 3 grouped launches (one plain launch per stage and line length over the tiles of all
+ * transforms in it, each kernel specialised for its line length), 4 the grouped launches
+ * replayed from a CUDA graph.  Modes 1-4 need float32. */
 int fftb_batch_exec(fftb_batch batch, int op, const void *in, void *out, double sign, int mode);
 /* error flag of the last persistent launch of op: 1 if a dependency wait ran out its
  * bounded number of polls (the launch then returned early); synchronises the device. */
@@ -264,9 +268,10 @@ int fftb_autotune_ffts(int dtype, long long nx, long long ny, long long nz, long
                        size_t *needed, int *from_cache);
 /* Applies the FFTB_AUTOTUNE_STRATEGY / _PLANE_CLUSTER of a config to an ffts object. */
 int fftb_ffts_apply_config(fftb_ffts obj, const char *text);
-/* load_or_measure for a batch and one op: candidates are sequential launches and the
- * graph-replayed persistent launch with tiles_scale {1, 2} x ctas_per_sm {0, 1, 2}.  The
- * winner's knobs are applied to the batch and its mode returned in *mode. */
+/* load_or_measure for a batch and one op: candidates are sequential launches, the
+ * graph-replayed persistent launch with tiles_scale {1, 2} x ctas_per_sm {0, 1, 2}, and
+ * the graph-replayed grouped launches with tiles_scale {1, 2}.  The winner's knobs are
+ * applied to the batch and its mode returned in *mode. */
 int fftb_autotune_batch(fftb_batch batch, int op, double sign, const char *cache_file, int flags, int warmup,
                         int iterations, char *text, size_t capacity, size_t *needed, int *from_cache, int *mode);
 /* Applies FFTB_AUTOTUNE_TILES_SCALE / _CTAS_PER_SM of a config; *mode = FFTB_AUTOTUNE_BATCH_MODE. */
