@@ -39,6 +39,14 @@ template <typename C> __device__ __forceinline__ C cmulc(C a, C b)
 }
 template <typename C> __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
 template <typename C, typename R> __device__ __forceinline__ C cscale(C a, R s) { a.x *= s; a.y *= s; return a; }
+
+// float2 forms on sm_100's paired FP32 instructions (FADD2 / FMUL2 / FFMA2: one
+// instruction for both components, each rounded as the scalar operation would be).
+// a - b is formed as fma(b, -1, a), which is exact in its product and so equals the
+// rounded difference.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
 // multiply by SIGN*i  (SIGN = -1: -i, SIGN = +1: +i)
 template <int SIGN, typename C> __device__ __forceinline__ C mul_si(C a)
 {
