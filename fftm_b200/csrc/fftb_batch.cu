@@ -170,6 +170,21 @@ bool batch_nf_supported(int nf)
     }
 }
 
+// Raises a kernel's dynamic shared-memory limit to the most the device allows beside its
+// static shared memory.  The limit belongs to the kernel, not to one plan: setting it to
+// one plan's need could lower it under the launches of another plan.
+cudaError_t raise_smem_limit(const void *fn)
+{
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    return e;
+}
+
 int floor_pow2(int v)
 {
     int p = 1;
@@ -391,13 +406,13 @@ int build_plan(fftb_batch_s *b, int op, double sign)
         if (e == cudaSuccess) e = cudaMemset(P.d_ctl, 0, (2 + P.npasses) * sizeof(int));
         if (e == cudaSuccess)
             e = cudaMemcpy(P.d_gitems, gitems.data(), gitems.size() * sizeof(BatchItem), cudaMemcpyHostToDevice);
+        // the limit is per kernel, not per plan: raise it to the maximum once, so a later
+        // plan with a smaller need cannot lower it under an earlier plan's launches
         for (const OpPlan::Group &g : P.groups)
-            if (e == cudaSuccess && g.smem > 48 * 1024)
-                e = cudaFuncSetAttribute(batch_group_fn(g.nf), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem);
+            if (e == cudaSuccess && g.smem > 48 * 1024) e = raise_smem_limit(batch_group_fn(g.nf));
         if (e != cudaSuccess) return set_status_from_cuda(e);
         if (smem > 48 * 1024) {
-            e = cudaFuncSetAttribute((const void *)batch_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem);
+            e = raise_smem_limit((const void *)batch_persistent_kernel);
             if (e != cudaSuccess) return set_status_from_cuda(e);
         }
         int dev = 0, sms = 0, occ = 0;

@@ -12,8 +12,66 @@
 
 #include "fftb_device.cuh"
 #include "fftb_internal.h"
+#include "fftb_regfft.cuh"
 
 namespace fftb {
+
+// Power-of-two lines of 32..256 points run the register-resident two-stage FFT
+// (fftb_regfft.cuh) on their staged line instead of the Stockham passes: one read of
+// the line into registers, radix-16 in registers, one exchange through the line's own
+// buffer, the second stage in registers, one write back.
+template <int NF> constexpr bool pass_regfft() { return NF >= 32 && NF <= 256 && (NF & (NF - 1)) == 0; }
+
+// pitch of a staged line: the padded line, or the register FFT's exchange region if larger
+template <int NF> constexpr int pass_line_pitch()
+{
+    return pass_regfft<NF>() && RegFFTShape<NF>::REGION > pad16(NF) + 1 ? RegFFTShape<NF>::REGION : pad16(NF) + 1;
+}
+
+// In-order FFT of the staged line `ln` (padded indices) by its T threads.  Every
+// thread of the block calls it; threads without a line (act == false) touch no shared
+// memory.  Ends with a block barrier.  tw: forward roots of length ntw (a multiple of NF).
+template <typename R, int NF, int SIGN>
+__device__ __forceinline__ void line_fft(cpx<R> *ln, cpx<R> *lnp, const cpx<R> *tw, int ntw, int t, bool act)
+{
+    if constexpr (pass_regfft<NF>()) {
+        using C = cpx<R>;
+        using S = RegFFTShape<NF>;
+        constexpr int T = S::T;
+        const unsigned mask = __activemask();
+        const int rs = ntw / NF;
+        C v[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) v[r] = act ? ln[pad16(t + T * r)] : mk<R>(R(0), R(0));
+        __syncwarp(mask);  // the line is read before the exchange overwrites it
+        dft16<SIGN, C, R>(v);
+#pragma unroll
+        for (int k1 = 1; k1 < 16; ++k1) v[k1] = twiddle_mul<SIGN>(v[k1], tw, (t * k1) * rs);
+        if (act) {
+#pragma unroll
+            for (int k1 = 0; k1 < 16; ++k1) ln[k1 * S::ROWP + t] = v[k1];
+        }
+        __syncwarp(mask);
+        constexpr int A = 16 / T;
+#pragma unroll
+        for (int a = 0; a < A; ++a) {
+            C u[T];
+#pragma unroll
+            for (int q = 0; q < T; ++q) u[q] = act ? ln[(t + T * a) * S::ROWP + q] : mk<R>(R(0), R(0));
+            dft_small<SIGN, T, C, R>(u);
+#pragma unroll
+            for (int k2 = 0; k2 < T; ++k2) v[a + A * k2] = u[k2];
+        }
+        __syncwarp(mask);  // the exchange region is read before the results overwrite it
+        if (act) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) ln[pad16(t + T * j)] = v[j];
+        }
+        __syncthreads();
+    } else {
+        fft_line<R, NF, SIGN>(lnp, tw, ntw, act ? t : 0, act);
+    }
+}
 
 template <typename R> __device__ __forceinline__ R ep_factor(const PassArgs &a, int p, const int *bidx)
 {
@@ -43,7 +101,7 @@ __device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, un
 {
     using C = cpx<R>;
     constexpr int T = threads_per_line(NF);
-    constexpr int LP = pad16(NF) + 1;
+    constexpr int LP = pass_line_pitch<NF>();
     C *stw_s = reinterpret_cast<C *>(smem_raw);
     const int ntw_s = a.tw_smem ? a.ntw : 0;
     long long *offs = reinterpret_cast<long long *>(stw_s + ntw_s);  // [G][2] in/out offsets
@@ -171,9 +229,9 @@ __device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, un
     // ------------------------------------------------------------ FFT core
     C *lnp = active_thread ? ln : lines;  // threads without a line still join the barriers
     if (kind == K_C2C_INV || kind == K_C2R) {
-        fft_line<R, NF, +1>(lnp, stw, a.ntw, active_thread ? t : 0, active_thread);
+        line_fft<R, NF, +1>(ln, lnp, stw, a.ntw, t, active_thread);
     } else {
-        fft_line<R, NF, -1>(lnp, stw, a.ntw, active_thread ? t : 0, active_thread);
+        line_fft<R, NF, -1>(ln, lnp, stw, a.ntw, t, active_thread);
     }
 
     if (kind == K_SANDWICH) {
@@ -181,7 +239,7 @@ __device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, un
             for (int p = t; p < NF; p += T) ln[pad16(p)] = cscale(ln[pad16(p)], ep_factor<R>(a, p, bidx + 4 * g));
         }
         __syncthreads();
-        fft_line<R, NF, +1>(lnp, stw, a.ntw, active_thread ? t : 0, active_thread);
+        line_fft<R, NF, +1>(ln, lnp, stw, a.ntw, t, active_thread);
     }
 
     // ------------------------------------------------------------ R2C post-processing
@@ -260,7 +318,7 @@ template <typename R, int NF> inline PassKernelInfo pass_kernel_info()
     PassKernelInfo k;
     k.nf = NF;
     k.threads_per_line = threads_per_line(NF);
-    k.line_pitch = pad16(NF) + 1;
+    k.line_pitch = pass_line_pitch<NF>();
     k.fn = (const void *)&fftb_pass_kernel<R, NF>;
     return k;
 }
