@@ -70,7 +70,7 @@ class Batch:
         self.real_total = rt.value
         self.spectrum_total = st.value
         self._work = None
-        self.mode = GRAPH
+        self.mode = GROUPED_GRAPH
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -109,7 +109,7 @@ class Batch:
 
     def exec(self, op, inp, out, sign=-1.0, mode=None, stream=None):
         """mode: SEQUENTIAL, PERSISTENT, GRAPH, GROUPED or GROUPED_GRAPH; None takes the
-        tuned mode (GRAPH if the batch was never tuned)."""
+        tuned mode (GROUPED_GRAPH if the batch was never tuned)."""
         if mode is None:
             mode = self.mode
         L = _lib.load()
