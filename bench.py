@@ -157,6 +157,32 @@ def ncu_traffic(kernel_name):
 
 
 # ---------------------------------------------------------------------- CPU legs
+def scipy_fft_rates(f_host):
+    """The same solve with scipy.fft on all host cores, float64 and float32 (a library
+    baseline beside the oracle; FFTW, the reference's CPU library, is not installed)."""
+    try:
+        import scipy.fft as sf
+    except Exception as exc:  # noqa: BLE001
+        return {"unavailable": str(exc)[:120]}
+    workers = os.cpu_count() or 1
+    k = np.fft.fftfreq(NX, 1.0 / NX)
+    kz = np.arange(NZ // 2 + 1)
+    k2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + kz[None, None, :] ** 2
+    with np.errstate(divide="ignore"):
+        mult = np.where(k2 == 0, 0.0, -1.0 / k2)
+    out = {"cores": workers}
+    for name, dt in (("f64", np.float64), ("f32", np.float32)):
+        x = f_host.astype(dt)
+        m = mult.astype(dt)
+        sf.irfftn(sf.rfftn(x, workers=workers) * m, s=x.shape, workers=workers)   # warm-up (plans)
+        t0 = time.perf_counter()
+        sf.irfftn(sf.rfftn(x, workers=workers) * m, s=x.shape, workers=workers)
+        dt_s = time.perf_counter() - t0
+        out[name] = {"seconds": dt_s, "value": BYTES_RT / dt_s / 1e9, "unit": "GB/s"}
+    return out
+
+
+
 def cpu_oracle_rate(f_host, sample_solves=1):
     """FP64 oracle Poisson solve on all host threads; returns (GB/s, seconds, threads, solution)."""
     import oracle as O
@@ -655,6 +681,7 @@ def main():
                                 "sample": "one full 256^3 FP64 Poisson solve (oracle/fft_oracle.c, OpenMP)",
                                 "seconds": secs}
         line["accuracy"] = {"rel_l2_vs_fp64_oracle": float(num / np.linalg.norm(ref.ravel()))}
+        line["cpu_scipy_fft"] = scipy_fft_rates(f_host)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
