@@ -3,7 +3,7 @@
 1. Dot-product identities <R2C x, G> = <x, R2C^T G> and <C2R Y, g> = <Y, C2R^T g>
    (real inner products, arbitrary complex G and Y) on every path: fused 3D, generic
    3D (odd sizes), 2D, and the three 4D layouts, f32 and f64.
-2. The differentiable pipeline of BASELINE config 4 at 128^3 f32: u = sin x cos y cos z
+2. The differentiable spectral pipeline at 128^3 f32: u = sin x cos y cos z
    + 0.05 N(0,1) (seed 4), w = Poisson(C2R(G(k) R2C(u)) / N) with the Gaussian
    G(k) = exp(-|k|^2 / (2 16^2)), loss = 0.5 ||w||^2.  Its gradient (adjoint kernels
    behind torch.autograd) is checked against torch autograd through torch.fft in
