@@ -75,7 +75,7 @@ template <int NY, int NZ, int CL, int NT_> struct PlaneShapeT {
     }
     template <typename R> static constexpr size_t smem_inv()
     {
-        return sizeof(cpx<R>) * ((size_t)M * PR + STG + TWS);
+        return sizeof(cpx<R>) * ((size_t)M * PR + STG + TWS + NY);  // + the staged kz = NZ/2 column
     }
     // CTAs per SM the register budget is sized for: 8-CTA clusters keep a CTA's shared
     // memory under a third of the SM's, so three CTAs (24 warps) fit when registers are
@@ -262,6 +262,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
     C *stg = rowsm + S::M * S::PR;                // column staging / FFT exchange regions
     C *twz = stg + S::STG;
     C *twy = twz + NZ;
+    C *nyq = twy + NY;                            // the kz = NZ/2 column (CTA 0 of a cluster)
     const int tid = threadIdx.x;
     const int c = (CL > 1) ? (int)cg::this_cluster().block_rank() : 0;
     const int x = (int)(blockIdx.x / CL);
@@ -289,6 +290,9 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
                 cp_async<sizeof(C)>(&buf[sl * S::PC + row],
                                     iplane + (size_t)row * (NZ / 2 + 1) + c * S::S + s0 + sl, true);
             }
+            if (c == 0 && s0 == 0)  // the packed slot's partner column, read by the first block
+                for (int row = tid; row < NY; row += S::NT)
+                    cp_async<sizeof(C)>(&nyq[row], iplane + (size_t)row * (NZ / 2 + 1) + NZ / 2, true);
             cp_async_commit();
         };
         stage(0, stg);
@@ -313,8 +317,8 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
                 for (int r = 0; r < 16; ++r) {
                     const int ky = t + TY * r, km = (NY - ky) & (NY - 1);
                     const C x0m = col[km];
-                    const C xnk = iplane[(size_t)ky * (NZ / 2 + 1) + NZ / 2];
-                    const C xnm = iplane[(size_t)km * (NZ / 2 + 1) + NZ / 2];
+                    const C xnk = nyq[ky];
+                    const C xnm = nyq[km];
                     const C h0 = cscale(cadd(v[r], cconj(x0m)), R(0.5));
                     const C hn = cscale(cadd(xnk, cconj(xnm)), R(0.5));
                     v[r] = mk<R>(h0.x - hn.y, h0.y + hn.x);
@@ -473,10 +477,12 @@ __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data,
         // rows of the transposed input -> shared memory -> columns in registers
         const C *src = tdata + (size_t)blockIdx.y * NX * ncols + (size_t)blockIdx.x * W * NX;
         const int nrow = (ncols - (int)blockIdx.x * W) < W ? (ncols - (int)blockIdx.x * W) : W;
+        // all of the tile's row loads in flight at once
         for (int e = tid; e < nrow * NX; e += 256) {
             const int rr = e / NX, kx = e - (e / NX) * NX;
-            scr[rr * RP + kx] = src[(size_t)rr * NX + kx];
+            cp_async<sizeof(C)>(&scr[rr * RP + kx], src + (size_t)rr * NX + kx, true);
         }
+        cp_async_wait_all();
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < 16; ++r) v[r] = scr[col * RP + t + T * r];
