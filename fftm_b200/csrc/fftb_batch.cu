@@ -1,4 +1,5 @@
-// fftb_batch.cu -- many 3D transforms of uneven sizes in one persistent launch.
+// fftb_batch.cu -- many 3D transforms of uneven sizes in one persistent launch or in
+// one launch per (stage, line length) group.
 //
 // Every transform of the batch is compiled into its pass program (the same passes
 // as a single ffts object).  The passes of all transforms are flattened into one
@@ -9,10 +10,14 @@
 // every tile of the previous pass of the same transform has been counted done.
 // Because items are taken in list order, every item a CTA waits for has already
 // been taken by a running CTA that waits only on items earlier still, so the wait
-// always ends; it is nevertheless bounded (FFTB_BATCH_SPIN_LIMIT polls), after
-// which the kernel raises an error flag that fftb_batch_status reports and every
-// CTA returns.  The launch (counter reset + kernel) is captured once into a CUDA
-// graph per buffer binding and replayed.
+// always ends; it is nevertheless bounded (kSpinLimit polls), after which the
+// kernel raises an error flag that fftb_batch_status reports and every CTA returns.
+// The launch (counter reset + kernel) is captured once into a CUDA graph per buffer
+// binding and replayed.
+//
+// The grouped form runs the same items as one plain launch per (stage, line length)
+// group, each a kernel specialised for its length, in stream order (no waits), and
+// can be replayed from a CUDA graph the same way.
 #include <cuda_runtime.h>
 
 #include <algorithm>

@@ -13,7 +13,7 @@
 //
 // All FFTs are register resident (fftb_regfft.cuh); shared memory holds the
 // plane between the z and y stages.  A plane too large for one CTA (a 256x256
-// plane is 133 KB of spectrum) is split over a cluster of 2 or 4 CTAs: each CTA
+// plane is 133 KB of spectrum) is split over a cluster of 2, 4 or 8 CTAs: each CTA
 // transforms a block of rows along z and owns a block of kz columns for the y
 // stage, and the data that changes owner in between is pushed into the owner's
 // shared memory with distributed-shared-memory stores, so no plane round-trips
@@ -34,7 +34,7 @@ namespace cg = cooperative_groups;
 namespace fftb {
 
 // ------------------------------------------------------------------ plane kernels
-// Work split (CL CTAs per plane, CL in {1, 2, 4}):
+// Work split (CL CTAs per plane, CL in {1, 2, 4, 8}):
 //   rows   : CTA c owns rows [c*M, (c+1)*M) for the z stage            (M = NY / CL)
 //   columns: CTA c owns column slots [c*S, (c+1)*S) for the y stage     (S = NZ / (2 CL))
 // Slot s < NZ/2 is spectrum column kz = s, except slot 0, which packs the two
