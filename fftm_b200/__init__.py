@@ -341,6 +341,19 @@ class ffts:
         _check(_lib.load().fftb_ffts_spectrum_poisson(self._h, _ptr(spectrum), float(sign), float(scale)),
                "spectrum_poisson")
 
+    def spectrum_derivative(self, spec_in, spec_out, axis, scale=1.0, stream=None):
+        """spec_out = i k_axis spec_in * scale (axis 0 = x, 1 = y, 2 = z, 3 = w)."""
+        self._ensure()
+        self._bind(stream)
+        _check(_lib.load().fftb_ffts_spectrum_derivative(self._h, _ptr(spec_in), _ptr(spec_out), int(axis),
+                                                         float(scale)), "spectrum_derivative")
+
+    def derivative(self, u, out, axis, stream=None):
+        """du/d(axis) of a periodic field on [0, 2 pi)^d (spectral, fused R2C / C2R)."""
+        self._ensure()
+        self._bind(stream)
+        _check(_lib.load().fftb_ffts_derivative(self._h, _ptr(u), _ptr(out), int(axis)), "derivative")
+
     def num_launches(self, which="forward") -> int:
         self._ensure()
         code = {"forward": 0, "backward": 1, "poisson": 2, "filter": 3}[which]

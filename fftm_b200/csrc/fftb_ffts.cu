@@ -31,6 +31,7 @@ struct fftb_ffts_s {
     Fused4D fused4;  // specialised 4D slab / native_xzwy kernels
     LaunchTimer timer;
     bool timing = false;
+    void *dspec = nullptr;  // spectrum buffer of fftb_ffts_derivative (allocated on first use)
 };
 
 namespace {
@@ -362,6 +363,61 @@ __global__ void spectrum_poisson_kernel(cpx<R> *s, long long total, int4 dims, i
     }
 }
 
+// out = i k_slot * in * scale: the spectral derivative of the reference's
+// derivative_spectra_functor (source/tests/test_3D_poisson.cu:113-145), with k = idx on
+// the half axis and k = idx <= n/2 ? idx : idx - n on the full axes (Nyquist kept, as there).
+template <typename R>
+__global__ void spectrum_derivative_kernel(const cpx<R> *in, cpx<R> *out, long long total, int4 dims, int4 ns,
+                                           int half_axis, int slot, R scale)
+{
+    const int d[4] = {dims.x, dims.y, dims.z, dims.w};
+    const int n[4] = {ns.x, ns.y, ns.z, ns.w};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long r = i;
+        int k = 0;
+#pragma unroll
+        for (int a = 3; a >= 0; --a) {
+            const int idx = (int)(r % d[a]);
+            r /= d[a];
+            if (a == slot) k = (a == half_axis) ? idx : (idx <= n[a] / 2 ? idx : idx - n[a]);
+        }
+        const cpx<R> v = in[i];
+        const R f = R(k) * scale;
+        cpx<R> w;
+        w.x = -f * v.y;
+        w.y = f * v.x;
+        out[i] = w;
+    }
+}
+
+// index geometry of the object's spectrum: slot extents, axis lengths, the half axis
+// slot, and the slot of each logical axis x, y, z, w
+void spectrum_geometry(const fftb_ffts_s *o, int4 &dims, int4 &ns, int &half_axis, int (&slot)[4])
+{
+    if (o->dim == 2) {
+        dims = make_int4(1, 1, (int)o->nx, (int)(o->ny / 2 + 1));
+        ns = make_int4(1, 1, (int)o->nx, (int)o->ny);
+        half_axis = 3;
+        slot[0] = 2; slot[1] = 3; slot[2] = slot[3] = -1;
+    } else if (o->dim == 3) {
+        dims = make_int4(1, (int)o->nx, (int)o->ny, (int)(o->nz / 2 + 1));
+        ns = make_int4(1, (int)o->nx, (int)o->ny, (int)o->nz);
+        half_axis = 3;
+        slot[0] = 1; slot[1] = 2; slot[2] = 3; slot[3] = -1;
+    } else if (o->layout == FFTB_4D_SLAB) {
+        dims = make_int4((int)o->nx, (int)o->ny, (int)o->nz, (int)(o->nw / 2 + 1));
+        ns = make_int4((int)o->nx, (int)o->ny, (int)o->nz, (int)o->nw);
+        half_axis = 3;
+        slot[0] = 0; slot[1] = 1; slot[2] = 2; slot[3] = 3;
+    } else {
+        dims = make_int4((int)o->ny, (int)o->nz, (int)(o->nw / 2 + 1), (int)o->nx);
+        ns = make_int4((int)o->ny, (int)o->nz, (int)o->nw, (int)o->nx);
+        half_axis = 2;
+        slot[0] = 3; slot[1] = 0; slot[2] = 1; slot[3] = 2;
+    }
+}
+
 } // namespace
 
 extern "C" {
@@ -399,6 +455,7 @@ int fftb_ffts_destroy(fftb_ffts o)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
     if (o->own_work && o->work) cudaFree(o->work);
+    if (o->dspec) cudaFree(o->dspec);
     delete o;
     return FFTB_SUCCESS;
 }
@@ -580,6 +637,49 @@ int fftb_ffts_spectrum_poisson(fftb_ffts o, void *spec, double sign, double scal
         spectrum_poisson_kernel<double><<<(unsigned)gs, bs, 0, o->stream>>>((double2 *)spec, total, dims, ns,
                                                                             half_axis, sign, scale);
     return set_status_from_cuda(cudaGetLastError());
+}
+
+int fftb_ffts_spectrum_derivative(fftb_ffts o, const void *spec_in, void *spec_out, int axis, double scale)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (!spec_in || !spec_out || axis < 0 || axis >= o->dim) return FFTB_ERROR_INVALID_VALUE;
+    int4 dims, ns;
+    int half_axis, slot[4];
+    spectrum_geometry(o, dims, ns, half_axis, slot);
+    const long long total = (long long)dims.x * dims.y * dims.z * dims.w;
+    const int bs = 256;
+    const long long gs = std::min<long long>((total + bs - 1) / bs, 148LL * 16);
+    if (o->dtype == FFTB_F32)
+        spectrum_derivative_kernel<float><<<(unsigned)gs, bs, 0, o->stream>>>(
+            (const float2 *)spec_in, (float2 *)spec_out, total, dims, ns, half_axis, slot[axis], (float)scale);
+    else
+        spectrum_derivative_kernel<double><<<(unsigned)gs, bs, 0, o->stream>>>(
+            (const double2 *)spec_in, (double2 *)spec_out, total, dims, ns, half_axis, slot[axis], scale);
+    return set_status_from_cuda(cudaGetLastError());
+}
+
+int fftb_ffts_derivative(fftb_ffts o, const void *in, void *out, int axis)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (!in || !out || axis < 0 || axis >= o->dim) return FFTB_ERROR_INVALID_VALUE;
+    if (!o->dspec) {
+        int4 dims, ns;
+        int half_axis, slot[4];
+        spectrum_geometry(o, dims, ns, half_axis, slot);
+        const size_t bytes = (size_t)dims.x * dims.y * dims.z * dims.w * complex_bytes(o->dtype);
+        if (cudaMalloc(&o->dspec, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            o->dspec = nullptr;
+            return FFTB_ERROR_ALLOC;
+        }
+    }
+    double n = (double)o->nx * (double)o->ny;
+    if (o->dim >= 3) n *= (double)o->nz;
+    if (o->dim == 4) n *= (double)o->nw;
+    int st = fftb_ffts_forward(o, in, o->dspec);
+    if (st == FFTB_SUCCESS) st = fftb_ffts_spectrum_derivative(o, o->dspec, o->dspec, axis, 1.0 / n);
+    if (st == FFTB_SUCCESS) st = fftb_ffts_backward(o, o->dspec, out);
+    return st;
 }
 
 int fftb_ffts_timing_enable(fftb_ffts o, int max_launches)

@@ -157,6 +157,14 @@ int fftb_ffts_backward_adjoint(fftb_ffts obj, const void *grad_real, void *grad_
  * reference's standalone functors): Poisson sign/|k|^2 (k=0 -> 0) with an extra
  * scale, examples/poisson/source/poisson_periodic_{3d,4d}_autotuned.cpp. */
 int fftb_ffts_spectrum_poisson(fftb_ffts obj, void *spectrum, double sign, double scale);
+/* Spectral derivative along a logical axis (0 = x, 1 = y, 2 = z, 3 = w) on a spectrum in
+ * this object's layout: spec_out = i k_axis spec_in * scale (the reference's
+ * derivative_spectra_functor, source/tests/test_3D_poisson.cu:113-145: k = index on the
+ * half axis, index or index - n on the full axes, Nyquist bins kept).  In place allowed. */
+int fftb_ffts_spectrum_derivative(fftb_ffts obj, const void *spec_in, void *spec_out, int axis, double scale);
+/* du/d(axis) of a periodic field on [0, 2 pi)^d: C2R(i k_axis R2C(u)) / N, through a
+ * spectrum buffer the object allocates on first use.  in and out may alias. */
+int fftb_ffts_derivative(fftb_ffts obj, const void *in, void *out, int axis);
 /* number of kernel launches of forward (which=0) / backward (1) / poisson (2) / filter (3) */
 int fftb_ffts_num_launches(fftb_ffts obj, int which, int *launches);
 /* Profiling hook (the role of the reference's ffts profiler, source/ffts.hpp:64-72,

@@ -1,0 +1,95 @@
+"""GPU tests of the spectral derivative (the reference's derivative_spectra_functor,
+source/tests/test_3D_poisson.cu:113-145: multiply by i k with k = index on the half axis
+and index or index - n on the full axes): the whole derivative du/d(axis) against the
+FP64 oracle pipeline and against analytic derivatives, and the standalone spectrum
+multiply on the 2D, 3D and 4D layouts against numpy."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def F(torch_cuda):
+    from fftm_b200 import build
+    build.build()
+    import fftm_b200
+    return fftm_b200
+
+
+def _k(n, half=False):
+    i = np.arange(n // 2 + 1 if half else n)
+    return i.astype(np.float64) if half else np.where(i <= n // 2, i, i - n).astype(np.float64)
+
+
+def _oracle_derivative(u, axis):
+    nx, ny, nz = u.shape
+    X = O.ffts3d_forward(u)
+    k = [_k(nx)[:, None, None], _k(ny)[None, :, None], _k(nz, True)[None, None, :]][axis]
+    return O.ffts3d_backward(1j * k * X, nz) / u.size
+
+
+@pytest.mark.parametrize("dtype,shape", [("float32", (64, 64, 64)), ("float32", (24, 20, 18)),
+                                         ("float64", (16, 12, 10)), ("float32", (32, 128, 256))])
+def test_derivative_vs_oracle(F, torch_cuda, dtype, shape):
+    torch = torch_cuda
+    rt = torch.float32 if dtype == "float32" else torch.float64
+    tol = 2e-6 if dtype == "float32" else 1e-12
+    u = O.random_3d(*shape, 17, single=(dtype == "float32"))
+    f = F.ffts(dtype).init(*shape)
+    ud = torch.tensor(u, dtype=rt, device="cuda")
+    out = torch.empty_like(ud)
+    for axis in range(3):
+        f.derivative(ud, out, axis)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy().astype(np.float64)
+        assert O.rel_l2(got, _oracle_derivative(u.astype(np.float64), axis)) <= tol, axis
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+def test_derivative_analytic(F, torch_cuda, dtype):
+    torch = torch_cuda
+    n = 32
+    g = 2 * np.pi * np.arange(n) / n
+    x, y, z = np.meshgrid(g, g, g, indexing="ij")
+    u = np.sin(x) * np.cos(2 * y) * np.sin(3 * z)
+    exact = [np.cos(x) * np.cos(2 * y) * np.sin(3 * z), -2 * np.sin(x) * np.sin(2 * y) * np.sin(3 * z),
+             3 * np.sin(x) * np.cos(2 * y) * np.cos(3 * z)]
+    rt = torch.float32 if dtype == "float32" else torch.float64
+    f = F.ffts(dtype).init(n, n, n)
+    ud = torch.tensor(u, dtype=rt, device="cuda")
+    out = torch.empty_like(ud)
+    for axis in range(3):
+        f.derivative(ud, out, axis)
+        torch.cuda.synchronize()
+        err = O.rel_l2(out.cpu().numpy().astype(np.float64), exact[axis])
+        assert err <= (2e-6 if dtype == "float32" else 1e-12), (axis, err)
+
+
+@pytest.mark.parametrize("dims,layout", [((12, 20), "pencil"), ((8, 6, 10, 12), "native_xzwy"),
+                                         ((8, 6, 10, 12), "slab"), ((8, 6, 10, 12), "pencil")])
+def test_spectrum_derivative_layouts(F, torch_cuda, dims, layout):
+    torch = torch_cuda
+    f = F.ffts("float64", strategy_4d=layout).init(*dims)
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal(f.spectrum_shape()) + 1j * rng.standard_normal(f.spectrum_shape())
+    Xd = torch.tensor(X, dtype=torch.complex128, device="cuda")
+    out = torch.empty_like(Xd)
+    d = len(dims)
+    # logical axis -> (physical axis of the spectrum, its length n, half axis?)
+    if d == 2:
+        phys = {0: (0, dims[0], False), 1: (1, dims[1], True)}
+    elif layout == "slab":
+        phys = {0: (0, dims[0], False), 1: (1, dims[1], False), 2: (2, dims[2], False), 3: (3, dims[3], True)}
+    else:  # [ky][kz][kw][kx]
+        phys = {0: (3, dims[0], False), 1: (0, dims[1], False), 2: (1, dims[2], False), 3: (2, dims[3], True)}
+    for axis in range(d):
+        f.spectrum_derivative(Xd, out, axis, 0.5)
+        torch.cuda.synchronize()
+        p, n, half = phys[axis]
+        shape = [1] * d
+        shape[p] = -1
+        ref = 0.5j * _k(n, half).reshape(shape) * X
+        assert O.rel_l2(out.cpu().numpy(), ref) <= 1e-14, axis
