@@ -348,6 +348,14 @@ class ffts:
         _check(_lib.load().fftb_ffts_spectrum_derivative(self._h, _ptr(spec_in), _ptr(spec_out), int(axis),
                                                          float(scale)), "spectrum_derivative")
 
+    def spectrum_truncate(self, spectrum, rule="two_thirds", cutoff=0, stream=None):
+        """Zero the modes outside |k_a| <= n_a / 3 ("two_thirds") or |k_a| <= cutoff ("box")."""
+        self._ensure()
+        self._bind(stream)
+        code = {"two_thirds": 0, "box": 1}[rule]
+        _check(_lib.load().fftb_ffts_spectrum_truncate(self._h, _ptr(spectrum), code, int(cutoff)),
+               "spectrum_truncate")
+
     def derivative(self, u, out, axis, stream=None):
         """du/d(axis) of a periodic field on [0, 2 pi)^d (spectral, fused R2C / C2R)."""
         self._ensure()

@@ -391,6 +391,38 @@ __global__ void spectrum_derivative_kernel(const cpx<R> *in, cpx<R> *out, long l
     }
 }
 
+// Zeroes the modes outside a box (the turbulence example's spectral truncations,
+// examples/turbulence/source/taylor_green_kernels.h:41-44, 186-200): rule 0 keeps
+// |k_a| <= n_a / 3 on every axis (two-thirds dealiasing), rule 1 keeps |k_a| <= cutoff
+// (cutoff <= 0 keeps everything).  k as in the derivative (signed on full axes).
+template <typename R>
+__global__ void spectrum_truncate_kernel(cpx<R> *s, long long total, int4 dims, int4 ns, int half_axis, int rule,
+                                         int cutoff)
+{
+    const int d[4] = {dims.x, dims.y, dims.z, dims.w};
+    const int n[4] = {ns.x, ns.y, ns.z, ns.w};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long r = i;
+        bool keep = true;
+#pragma unroll
+        for (int a = 3; a >= 0; --a) {
+            const int idx = (int)(r % d[a]);
+            r /= d[a];
+            if (n[a] <= 1) continue;  // unused slot
+            const int k = (a == half_axis) ? idx : (idx <= n[a] / 2 ? idx : idx - n[a]);
+            const int ak = k < 0 ? -k : k;
+            if (rule == 0 ? ak > n[a] / 3 : (cutoff > 0 && ak > cutoff)) keep = false;
+        }
+        if (!keep) {
+            cpx<R> z;
+            z.x = R(0);
+            z.y = R(0);
+            s[i] = z;
+        }
+    }
+}
+
 // index geometry of the object's spectrum: slot extents, axis lengths, the half axis
 // slot, and the slot of each logical axis x, y, z, w
 void spectrum_geometry(const fftb_ffts_s *o, int4 &dims, int4 &ns, int &half_axis, int (&slot)[4])
@@ -655,6 +687,25 @@ int fftb_ffts_spectrum_derivative(fftb_ffts o, const void *spec_in, void *spec_o
     else
         spectrum_derivative_kernel<double><<<(unsigned)gs, bs, 0, o->stream>>>(
             (const double2 *)spec_in, (double2 *)spec_out, total, dims, ns, half_axis, slot[axis], scale);
+    return set_status_from_cuda(cudaGetLastError());
+}
+
+int fftb_ffts_spectrum_truncate(fftb_ffts o, void *spec, int rule, int cutoff)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (!spec || (rule != FFTB_TRUNCATE_TWO_THIRDS && rule != FFTB_TRUNCATE_BOX)) return FFTB_ERROR_INVALID_VALUE;
+    int4 dims, ns;
+    int half_axis, slot[4];
+    spectrum_geometry(o, dims, ns, half_axis, slot);
+    const long long total = (long long)dims.x * dims.y * dims.z * dims.w;
+    const int bs = 256;
+    const long long gs = std::min<long long>((total + bs - 1) / bs, 148LL * 16);
+    if (o->dtype == FFTB_F32)
+        spectrum_truncate_kernel<float><<<(unsigned)gs, bs, 0, o->stream>>>((float2 *)spec, total, dims, ns,
+                                                                            half_axis, rule, cutoff);
+    else
+        spectrum_truncate_kernel<double><<<(unsigned)gs, bs, 0, o->stream>>>((double2 *)spec, total, dims, ns,
+                                                                             half_axis, rule, cutoff);
     return set_status_from_cuda(cudaGetLastError());
 }
 

@@ -162,6 +162,13 @@ int fftb_ffts_spectrum_poisson(fftb_ffts obj, void *spectrum, double sign, doubl
  * derivative_spectra_functor, source/tests/test_3D_poisson.cu:113-145: k = index on the
  * half axis, index or index - n on the full axes, Nyquist bins kept).  In place allowed. */
 int fftb_ffts_spectrum_derivative(fftb_ffts obj, const void *spec_in, void *spec_out, int axis, double scale);
+/* Spectral truncation in place (the turbulence example's filters,
+ * examples/turbulence/source/taylor_green_kernels.h:41-44, 186-200): TWO_THIRDS keeps
+ * |k_a| <= n_a / 3 on every axis (dealiasing), BOX keeps |k_a| <= cutoff (cutoff <= 0
+ * keeps all); every other mode is set to 0.  k as in fftb_ffts_spectrum_derivative. */
+#define FFTB_TRUNCATE_TWO_THIRDS 0
+#define FFTB_TRUNCATE_BOX 1
+int fftb_ffts_spectrum_truncate(fftb_ffts obj, void *spectrum, int rule, int cutoff);
 /* du/d(axis) of a periodic field on [0, 2 pi)^d: C2R(i k_axis R2C(u)) / N, through a
  * spectrum buffer the object allocates on first use.  in and out may alias. */
 int fftb_ffts_derivative(fftb_ffts obj, const void *in, void *out, int axis);

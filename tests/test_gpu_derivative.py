@@ -93,3 +93,33 @@ def test_spectrum_derivative_layouts(F, torch_cuda, dims, layout):
         shape[p] = -1
         ref = 0.5j * _k(n, half).reshape(shape) * X
         assert O.rel_l2(out.cpu().numpy(), ref) <= 1e-14, axis
+
+
+@pytest.mark.parametrize("dims,layout", [((24, 18, 30), "pencil"), ((8, 6, 10, 12), "native_xzwy"),
+                                         ((12, 20), "pencil")])
+@pytest.mark.parametrize("rule,cutoff", [("two_thirds", 0), ("box", 3), ("box", 0)])
+def test_spectrum_truncate(F, torch_cuda, dims, layout, rule, cutoff):
+    torch = torch_cuda
+    f = F.ffts("float32", strategy_4d=layout).init(*dims)
+    rng = np.random.default_rng(9)
+    X = (rng.standard_normal(f.spectrum_shape()) + 1j * rng.standard_normal(f.spectrum_shape())).astype(np.complex64)
+    Xd = torch.tensor(X, device="cuda")
+    f.spectrum_truncate(Xd, rule, cutoff)
+    torch.cuda.synchronize()
+    d = len(dims)
+    if d == 2:
+        axes = [(0, dims[0], False), (1, dims[1], True)]
+    elif d == 3:
+        axes = [(0, dims[0], False), (1, dims[1], False), (2, dims[2], True)]
+    else:  # [ky][kz][kw][kx]
+        axes = [(3, dims[0], False), (0, dims[1], False), (1, dims[2], False), (2, dims[3], True)]
+    keep = np.ones(f.spectrum_shape(), bool)
+    for p, n, half in axes:
+        shape = [1] * d
+        shape[p] = -1
+        ak = np.abs(_k(n, half)).reshape(shape)
+        if rule == "two_thirds":
+            keep &= ak <= n // 3
+        elif cutoff > 0:
+            keep &= ak <= cutoff
+    np.testing.assert_array_equal(Xd.cpu().numpy(), np.where(keep, X, 0))
