@@ -337,7 +337,7 @@ int build_plan(fftb_batch_s *b, int op, double sign)
         const Launch &L = P.seq.launches[p];
         PassArgs a = L.args;
         const int T = L.k.threads_per_line;
-        if (!batch_nf_supported(L.k.nf)) P.persistent_ok = false;
+        if (!batch_nf_supported(L.k.nf) || a.bs_n != 0) P.persistent_ok = false;  // chirp-z lines: sequential
         int G = std::min(a.G, floor_pow2(std::max(1, kBatchThreads / T)));
         G = std::max(1, G / b->tiles_scale);
         a.G = G;

@@ -1,5 +1,6 @@
 // fftb_engine.cu -- kernel registry, twiddle tables, program builder / executor.
 #include "fftb_engine.h"
+#include "fftb_bluestein.h"
 
 #include <algorithm>
 #include <cstring>
@@ -152,16 +153,32 @@ int program_add(Program &prog, int dtype, const AxisPass &p)
     memset(&L.args, 0, sizeof(L.args));
     PassArgs &a = L.args;
     const bool realk = (p.kind == K_R2C || p.kind == K_C2R);
-    const bool half = realk && (p.n % 2 == 0);
-    const int nf = half ? p.n / 2 : p.n;
+    bool half = realk && (p.n % 2 == 0);
+    int nf = half ? p.n / 2 : p.n;
     Registry &r = reg();
     auto it = r.tab[dtype].find(nf);
-    if (it == r.tab[dtype].end()) {
+    if (it == r.tab[dtype].end() && half) {
+        // no half-length kernel: the real line as a full complex line
+        half = false;
+        nf = p.n;
+        it = r.tab[dtype].find(nf);
+    }
+    bool chirpz = false;
+    if (it != r.tab[dtype].end()) {
+        L.k = it->second;
+    } else if (bluestein_kernel(dtype, p.n, &L.k)) {
+        chirpz = true;   // L.k.nf is the convolution length
+        const void *ch = nullptr, *bh = nullptr;
+        int st = bluestein_tables(dtype, p.n, &ch, &bh);
+        if (st != FFTB_SUCCESS) return st;
+        a.bs_n = p.n;
+        a.bs_chirp = ch;
+        a.bs_bhat = bh;
+    } else {
         set_last_error("no kernel for line length " + std::to_string(p.n));
         return FFTB_ERROR_UNSUPPORTED_SIZE;
     }
-    L.k = it->second;
-    const int ntw = half ? 2 * nf : nf;
+    const int ntw = chirpz ? L.k.nf : (half ? 2 * nf : nf);
     void *roots = nullptr;
     int st = get_roots(dtype, ntw, &roots);
     if (st != FFTB_SUCCESS) return st;
@@ -283,8 +300,8 @@ int program_add(Program &prog, int dtype, const AxisPass &p)
         const long long pin = (p.kind == K_C2R) ? (long long)(p.n / 2 + 1) : (long long)p.n;
         const long long pout = (p.kind == K_R2C) ? (long long)(p.n / 2 + 1) : (long long)p.n;
         L.alg_bytes = (double)nlines * ((double)pin * (double)in_el + (double)pout * (double)out_el);
-        L.name = std::string("fftb_pass_kernel<") + (dtype == 0 ? "f32" : "f64") + "," + std::to_string(nf) + ">/" +
-                 kn[p.kind] + "/n" + std::to_string(p.n);
+        L.name = std::string(chirpz ? "fftb_bluestein_kernel<" : "fftb_pass_kernel<") + (dtype == 0 ? "f32" : "f64") +
+                 "," + std::to_string(chirpz ? L.k.nf : nf) + ">/" + kn[p.kind] + "/n" + std::to_string(p.n);
     }
     prog.dtype = dtype;
     prog.launches.push_back(L);

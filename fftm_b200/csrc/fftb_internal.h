@@ -49,6 +49,10 @@ struct PassArgs {
     int ep_half[4];
     double ep_kscale[4];
     double ep_scale, ep_sign, ep_gauss, ep_hw;
+    // chirp-z passes (bs_n > 0): line length n, chirp table (n) and convolution
+    // kernel spectrum (M); tw / ntw are then the roots of the convolution length M
+    int bs_n;
+    const void *bs_chirp, *bs_bhat;
 };
 
 struct PassKernelInfo {

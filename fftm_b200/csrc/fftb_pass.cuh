@@ -216,9 +216,10 @@ __device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, un
                     if (k != 0) ln[pad16(NF - k)] = cconj(csub(e, io));
                 }
             } else {
-                // odd length: Hermitian extension of the half line
+                // full-length line: Hermitian extension of the half line (the imaginary
+                // parts of the DC and, for even lengths, Nyquist bins are ignored)
                 for (int k = t; k < NF; k += T) {
-                    if (k == 0) { C v = ln[0]; v.y = R(0); ln[0] = v; }
+                    if (k == 0 || 2 * k == NF) { C v = ln[pad16(k)]; v.y = R(0); ln[pad16(k)] = v; }
                     else if (k > NF / 2) ln[pad16(k)] = cconj(ln[pad16(NF - k)]);
                 }
             }
