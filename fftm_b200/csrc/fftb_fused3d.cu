@@ -629,11 +629,21 @@ const XColEntry *find_xcol(int dtype, int nx)
     return nullptr;
 }
 
+// Raises the kernel's dynamic shared-memory limit to what the device allows beside its
+// static shared memory (once for all uses: a per-use value could lower it under another
+// object's launches of the same kernel).
 int configure(const void *fn, size_t smem)
 {
-    if (smem > 48 * 1024)
-        return set_status_from_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    return FFTB_SUCCESS;
+    if (smem <= 48 * 1024) return FFTB_SUCCESS;
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
+    if (e == cudaSuccess && smem + fa.sharedSizeBytes > (size_t)optin) return FFTB_ERROR_UNSUPPORTED_SIZE;
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    return set_status_from_cuda(e);
 }
 
 // One launch of a plane kernel over `nplanes` planes.
