@@ -348,6 +348,15 @@ class ffts:
         _check(_lib.load().fftb_ffts_spectrum_derivative(self._h, _ptr(spec_in), _ptr(spec_out), int(axis),
                                                          float(scale)), "spectrum_derivative")
 
+    def gradient(self, u, outs, stream=None):
+        """outs[a] = du/d(axis a) for every axis, from one forward transform."""
+        self._ensure()
+        self._bind(stream)
+        if len(outs) != len(self._dims):
+            raise ValueError(f"gradient needs {len(self._dims)} outputs")
+        arr = (ctypes.c_void_p * len(outs))(*[_ptr(o) for o in outs])
+        _check(_lib.load().fftb_ffts_gradient(self._h, _ptr(u), arr), "gradient")
+
     def spectrum_truncate(self, spectrum, rule="two_thirds", cutoff=0, stream=None):
         """Zero the modes outside |k_a| <= n_a / 3 ("two_thirds") or |k_a| <= cutoff ("box")."""
         self._ensure()

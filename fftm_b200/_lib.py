@@ -27,7 +27,7 @@ EXPORTS = [
     "fftb_ffts_set_strategy", "fftb_ffts_get_strategy",
     "fftb_autotune_load_file", "fftb_autotune_save_file", "fftb_autotune_validate", "fftb_autotune_hardware",
     "fftb_autotune_ffts", "fftb_ffts_apply_config", "fftb_autotune_batch", "fftb_batch_apply_config",
-    "fftb_ffts_spectrum_derivative", "fftb_ffts_derivative", "fftb_ffts_spectrum_truncate",
+    "fftb_ffts_spectrum_derivative", "fftb_ffts_derivative", "fftb_ffts_spectrum_truncate", "fftb_ffts_gradient",
 ]
 
 _lib = None
@@ -103,6 +103,7 @@ def load():
     L.fftb_ffts_spectrum_derivative.argtypes = [c_vp, c_vp, c_vp, c_int, c_d]
     L.fftb_ffts_derivative.argtypes = [c_vp, c_vp, c_vp, c_int]
     L.fftb_ffts_spectrum_truncate.argtypes = [c_vp, c_vp, c_int, c_int]
+    L.fftb_ffts_gradient.argtypes = [c_vp, c_vp, ctypes.POINTER(c_vp)]
     for name in EXPORTS:
         if name not in ("fftb_status_string", "fftb_version", "fftb_last_error_message"):
             getattr(L, name).restype = c_int

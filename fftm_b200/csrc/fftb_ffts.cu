@@ -31,7 +31,8 @@ struct fftb_ffts_s {
     Fused4D fused4;  // specialised 4D slab / native_xzwy kernels
     LaunchTimer timer;
     bool timing = false;
-    void *dspec = nullptr;  // spectrum buffer of fftb_ffts_derivative (allocated on first use)
+    void *dspec = nullptr;  // spectrum buffers of the derivative calls (allocated on first use)
+    void *dspec2 = nullptr;
 };
 
 namespace {
@@ -488,6 +489,7 @@ int fftb_ffts_destroy(fftb_ffts o)
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
     if (o->own_work && o->work) cudaFree(o->work);
     if (o->dspec) cudaFree(o->dspec);
+    if (o->dspec2) cudaFree(o->dspec2);
     delete o;
     return FFTB_SUCCESS;
 }
@@ -709,27 +711,61 @@ int fftb_ffts_spectrum_truncate(fftb_ffts o, void *spec, int rule, int cutoff)
     return set_status_from_cuda(cudaGetLastError());
 }
 
+} // extern "C"
+
+namespace {
+int ensure_spectrum(fftb_ffts_s *o, void **buf)
+{
+    if (*buf) return FFTB_SUCCESS;
+    int4 dims, ns;
+    int half_axis, slot[4];
+    spectrum_geometry(o, dims, ns, half_axis, slot);
+    const size_t bytes = (size_t)dims.x * dims.y * dims.z * dims.w * complex_bytes(o->dtype);
+    if (cudaMalloc(buf, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        *buf = nullptr;
+        return FFTB_ERROR_ALLOC;
+    }
+    return FFTB_SUCCESS;
+}
+
+double points(const fftb_ffts_s *o)
+{
+    double n = (double)o->nx * (double)o->ny;
+    if (o->dim >= 3) n *= (double)o->nz;
+    if (o->dim == 4) n *= (double)o->nw;
+    return n;
+}
+} // namespace
+
+extern "C" {
+
 int fftb_ffts_derivative(fftb_ffts o, const void *in, void *out, int axis)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
     if (!in || !out || axis < 0 || axis >= o->dim) return FFTB_ERROR_INVALID_VALUE;
-    if (!o->dspec) {
-        int4 dims, ns;
-        int half_axis, slot[4];
-        spectrum_geometry(o, dims, ns, half_axis, slot);
-        const size_t bytes = (size_t)dims.x * dims.y * dims.z * dims.w * complex_bytes(o->dtype);
-        if (cudaMalloc(&o->dspec, bytes) != cudaSuccess) {
-            cudaGetLastError();
-            o->dspec = nullptr;
-            return FFTB_ERROR_ALLOC;
-        }
-    }
-    double n = (double)o->nx * (double)o->ny;
-    if (o->dim >= 3) n *= (double)o->nz;
-    if (o->dim == 4) n *= (double)o->nw;
-    int st = fftb_ffts_forward(o, in, o->dspec);
-    if (st == FFTB_SUCCESS) st = fftb_ffts_spectrum_derivative(o, o->dspec, o->dspec, axis, 1.0 / n);
+    int st = ensure_spectrum(o, &o->dspec);
+    if (st == FFTB_SUCCESS) st = fftb_ffts_forward(o, in, o->dspec);
+    if (st == FFTB_SUCCESS) st = fftb_ffts_spectrum_derivative(o, o->dspec, o->dspec, axis, 1.0 / points(o));
     if (st == FFTB_SUCCESS) st = fftb_ffts_backward(o, o->dspec, out);
+    return st;
+}
+
+int fftb_ffts_gradient(fftb_ffts o, const void *in, void *const *outs)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (!in || !outs) return FFTB_ERROR_INVALID_VALUE;
+    for (int a = 0; a < o->dim; ++a)
+        if (!outs[a]) return FFTB_ERROR_INVALID_VALUE;
+    int st = ensure_spectrum(o, &o->dspec);
+    if (st == FFTB_SUCCESS) st = ensure_spectrum(o, &o->dspec2);
+    // one forward transform; per axis the i k multiply into the second buffer (the
+    // backward transform consumes its input) and the backward transform
+    if (st == FFTB_SUCCESS) st = fftb_ffts_forward(o, in, o->dspec);
+    for (int a = 0; a < o->dim && st == FFTB_SUCCESS; ++a) {
+        st = fftb_ffts_spectrum_derivative(o, o->dspec, o->dspec2, a, 1.0 / points(o));
+        if (st == FFTB_SUCCESS) st = fftb_ffts_backward(o, o->dspec2, outs[a]);
+    }
     return st;
 }
 

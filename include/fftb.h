@@ -172,6 +172,10 @@ int fftb_ffts_spectrum_truncate(fftb_ffts obj, void *spectrum, int rule, int cut
 /* du/d(axis) of a periodic field on [0, 2 pi)^d: C2R(i k_axis R2C(u)) / N, through a
  * spectrum buffer the object allocates on first use.  in and out may alias. */
 int fftb_ffts_derivative(fftb_ffts obj, const void *in, void *out, int axis);
+/* Every first derivative of u from one forward transform (the reference test's dx, dy,
+ * dz spectra, source/tests/test_3D_poisson.cu:113-145): outs[a] = du/d(axis a) for the
+ * object's dim axes (x, y, z[, w]); each output is a real array of the input's shape. */
+int fftb_ffts_gradient(fftb_ffts obj, const void *in, void *const *outs);
 /* number of kernel launches of forward (which=0) / backward (1) / poisson (2) / filter (3) */
 int fftb_ffts_num_launches(fftb_ffts obj, int which, int *launches);
 /* Profiling hook (the role of the reference's ffts profiler, source/ffts.hpp:64-72,
