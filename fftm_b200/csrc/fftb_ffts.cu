@@ -641,26 +641,8 @@ int fftb_ffts_spectrum_poisson(fftb_ffts o, void *spec, double sign, double scal
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
     if (!spec) return FFTB_ERROR_INVALID_VALUE;
     int4 dims, ns;
-    int half_axis;
-    const int nxh = 0;
-    (void)nxh;
-    if (o->dim == 2) {
-        dims = make_int4(1, 1, (int)o->nx, (int)(o->ny / 2 + 1));
-        ns = make_int4(1, 1, (int)o->nx, (int)o->ny);
-        half_axis = 3;
-    } else if (o->dim == 3) {
-        dims = make_int4(1, (int)o->nx, (int)o->ny, (int)(o->nz / 2 + 1));
-        ns = make_int4(1, (int)o->nx, (int)o->ny, (int)o->nz);
-        half_axis = 3;
-    } else if (o->layout == FFTB_4D_SLAB) {
-        dims = make_int4((int)o->nx, (int)o->ny, (int)o->nz, (int)(o->nw / 2 + 1));
-        ns = make_int4((int)o->nx, (int)o->ny, (int)o->nz, (int)o->nw);
-        half_axis = 3;
-    } else {
-        dims = make_int4((int)o->ny, (int)o->nz, (int)(o->nw / 2 + 1), (int)o->nx);
-        ns = make_int4((int)o->ny, (int)o->nz, (int)o->nw, (int)o->nx);
-        half_axis = 2;
-    }
+    int half_axis, slot[4];
+    spectrum_geometry(o, dims, ns, half_axis, slot);
     const long long total = (long long)dims.x * dims.y * dims.z * dims.w;
     const int bs = 256;
     const long long gs = std::min<long long>((total + bs - 1) / bs, 148LL * 16);
