@@ -96,3 +96,27 @@ def test_batch_full_workload_512(B, torch_cuda):
     assert b.status(B.ROUNDTRIP) == 0
     assert float(torch.linalg.norm(out - x) / torch.linalg.norm(x)) <= TOL
 
+
+
+def test_batch_float64_runs_sequential_launches(B, torch_cuda):
+    torch = torch_cuda
+    shapes = [(16, 12, 10), (9, 8, 14), (32, 16, 8)]
+    b = B.Batch(shapes, dtype="float64")
+    assert b.describe(B.ROUNDTRIP)["persistent"] == 0
+    x = torch.rand(b.real_total, dtype=torch.float64, device="cuda") * 2 - 1
+    for mode in (B.SEQUENTIAL, B.GRAPH, B.GROUPED_GRAPH):   # float64 runs the plain launches in every mode
+        out = torch.zeros_like(x)
+        b.exec(B.ROUNDTRIP, x, out, mode=mode)
+        torch.cuda.synchronize()
+        for i, s in enumerate(shapes):
+            o = b.real_offsets[i]
+            n = int(np.prod(s))
+            assert O.rel_l2(out[o:o + n].cpu().numpy(), x[o:o + n].cpu().numpy()) <= 1e-12
+
+
+def test_tensor_core_form_needs_float32(B, torch_cuda):
+    import fftm_b200 as F
+    f = F.ffts("float64").init(64, 64, 64)
+    with pytest.raises(F.FftbError) as e:
+        f.set_strategy("fused_tc")
+    assert e.value.status == -2
