@@ -727,7 +727,10 @@ int fftb_ffts_derivative(fftb_ffts o, const void *in, void *out, int axis)
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
     if (!in || !out || axis < 0 || axis >= o->dim) return FFTB_ERROR_INVALID_VALUE;
     int st = ensure_spectrum(o, &o->dspec);
-    if (st == FFTB_SUCCESS) st = fftb_ffts_forward(o, in, o->dspec);
+    if (st != FFTB_SUCCESS) return st;
+    if (o->fused.enabled && aligned16(in, out))  // the multiply rides in the x column pass
+        return fused3d_derivative(o->fused, in, o->dspec, out, axis, o->stream, o->timing ? &o->timer : nullptr);
+    st = fftb_ffts_forward(o, in, o->dspec);
     if (st == FFTB_SUCCESS) st = fftb_ffts_spectrum_derivative(o, o->dspec, o->dspec, axis, 1.0 / points(o));
     if (st == FFTB_SUCCESS) st = fftb_ffts_backward(o, o->dspec, out);
     return st;

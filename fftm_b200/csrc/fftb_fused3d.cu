@@ -410,6 +410,10 @@ struct XColEp {
     float hw_f;
     double hw;
     int tc;  // host side: launch the tensor-core variant of the kernel
+    // EP_DERIV (3D, inverse mode): multiply by i k_daxis * dscale before the x FFT
+    int daxis;
+    float dscale_f;
+    double dscale;
 };
 
 template <int NX> struct XColShape {
@@ -510,7 +514,19 @@ __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data,
         const R kyz = R(ky * ky + kz * kz + kw * kw);
         const R sc = sizeof(R) == 4 ? R(ep.scale_f) : R(ep.scale);
         const R sg = sizeof(R) == 4 ? R(ep.sign_f) : R(ep.sign);
-        if ((ep.mode & (EP_POISSON | EP_GAUSS)) == EP_POISSON) {
+        if (ep.mode & EP_DERIV) {
+            // i k v * scale with k = kx (row), ky or kz (the column); 3D only.  kz is the half
+            // axis: its Nyquist bin carries the real cosine part, whose derivative the C2R
+            // drops with the imaginary part, the same as a separate multiply does
+            const R ds = sizeof(R) == 4 ? R(ep.dscale_f) : R(ep.dscale);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int kxi = t + T * j;
+                const int k = ep.daxis == 0 ? (kxi <= NX / 2 ? kxi : kxi - NX) : (ep.daxis == 1 ? ky : kz);
+                const R fct = R(k) * ds;
+                v[j] = mk<R>(-fct * v[j].y, fct * v[j].x);
+            }
+        } else if ((ep.mode & (EP_POISSON | EP_GAUSS)) == EP_POISSON) {
             const R ss = sc * sg;
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
@@ -824,6 +840,32 @@ int fused3d_spectral(const Fused3D &f, const void *in, void *out, void *work, co
     if (st == FFTB_SUCCESS) st = launch_xcol(f, 2, work, &ep, s, t);
     if (st == FFTB_SUCCESS)
         st = launch_plane(f, true, work, out, 1.0 / (double)(f.nx * f.ny * f.nz), s, t);
+    if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
+    return st;
+}
+
+// du/d(axis): plane R2C into spec, the x column sandwich (forward, i k, inverse) in place,
+// the inverse planes with 1/N
+int fused3d_derivative(const Fused3D &f, const void *in, void *spec, void *out, int axis, cudaStream_t s,
+                       LaunchTimer *t)
+{
+    const long long nzh = f.nz / 2 + 1;
+    int st = launch_plane(f, false, in, spec, 1.0, s, t);
+    if (st == FFTB_SUCCESS) {
+        XColEp x = make_ep(nullptr);
+        x.mode = EP_DERIV;
+        x.daxis = axis;
+        x.dscale = 1.0;
+        x.dscale_f = 1.f;
+        x.nzh = (int)nzh;
+        x.ny = (int)f.ny;
+        x.nz = (int)f.nz;
+        x.hn = (int)f.nz;
+        x.tc = f.tc ? 1 : 0;
+        st = launch_xcol_n((const XColEntry *)f.xcol, 2, spec, f.ny * nzh, f.ny * nzh, 1, 0, nullptr, f.roots_x, x, s,
+                           t);
+    }
+    if (st == FFTB_SUCCESS) st = launch_plane(f, true, spec, out, 1.0 / (double)(f.nx * f.ny * f.nz), s, t);
     if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
     return st;
 }

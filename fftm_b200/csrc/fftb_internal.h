@@ -22,6 +22,7 @@ enum EpMode : int {
     EP_POISSON = 2,  // multiply by ep_sign / |k|^2 (0 at k = 0)
     EP_GAUSS = 4,    // multiply by exp(-|k|^2 * ep_gauss)
     EP_HALFW = 8,    // multiply interior bins of the half (R2C) axis by ep_hw (adjoint weights)
+    EP_DERIV = 16,   // multiply by i k_axis * scale (spectral derivative; fused column kernel)
 };
 
 // Everything one pass launch needs.  POD, passed by value.

@@ -127,15 +127,17 @@ def test_spectrum_truncate(F, torch_cuda, dims, layout, rule, cutoff):
 
 @pytest.mark.parametrize("dtype,shape,layout", [("float32", (64, 64, 64), "pencil"), ("float64", (15, 12, 17), "pencil"),
                                                 ("float64", (6, 8, 10, 12), "native_xzwy")])
-def test_gradient_equals_derivatives(F, torch_cuda, dtype, shape, layout):
+def test_gradient_matches_derivatives(F, torch_cuda, dtype, shape, layout):
     torch = torch_cuda
     rt = torch.float32 if dtype == "float32" else torch.float64
     f = F.ffts(dtype, strategy_4d=layout).init(*shape)
     u = torch.randn(f.real_shape(), dtype=rt, device="cuda")
     outs = [torch.empty_like(u) for _ in shape]
     f.gradient(u, outs)
+    tol = 2e-6 if dtype == "float32" else 1e-12
     for a in range(len(shape)):
         ref = torch.empty_like(u)
-        f.derivative(u, ref, a)
+        f.derivative(u, ref, a)       # on the fused path the multiply rides in the column pass
         torch.cuda.synchronize()
-        assert torch.equal(outs[a], ref), a
+        err = float(torch.linalg.norm((outs[a] - ref).double()) / torch.linalg.norm(ref.double()))
+        assert err <= tol, (a, err)
