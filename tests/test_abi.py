@@ -92,3 +92,29 @@ def test_library_has_no_cufft_dependency(lib):
     from fftm_b200 import _lib
     out = subprocess.run(["ldd", _lib.LIB_PATH], capture_output=True, text=True).stdout
     assert "cufft" not in out
+
+
+def _build_cpp_example(lib_path, exe):
+    """Compiles tests/cpp_api_example.cpp against include/fftb.hpp and links it to the
+    library (g++, C++17)."""
+    import subprocess
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    libdir = os.path.dirname(lib_path)
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror", "-o", str(exe),
+           os.path.join(ROOT, "tests", "cpp_api_example.cpp"), "-I" + os.path.join(ROOT, "include"),
+           "-I" + os.path.join(cuda, "include"), "-L" + libdir, "-lfftb_b200", "-L" + os.path.join(cuda, "lib64"),
+           "-lcudart", "-Wl,-rpath," + libdir + ":" + os.path.join(cuda, "lib64")]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+
+
+def test_cpp_header_layer_host_checks(lib, tmp_path):
+    # include/fftb.hpp compiles warning-free and its host-side logic (status -> exception
+    # mapping, KEY=VALUE text, option flags) runs without a GPU
+    import subprocess
+    from fftm_b200 import _lib
+    exe = tmp_path / "cpp_api_example"
+    _build_cpp_example(_lib.LIB_PATH, exe)
+    p = subprocess.run([str(exe), "--host-only"], capture_output=True, text=True, timeout=60)
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert p.stdout.strip().endswith("ok")
+    assert "FAIL" not in p.stdout

@@ -1,6 +1,8 @@
 """The C ABI from a plain C program (tests/c_abi_example.c): compiled with gcc against
 include/fftb.h and linked to libfftb_b200.so, it solves a manufactured Poisson problem,
-checks a round trip, runs a plan and an error path -- no Python or torch in between."""
+checks a round trip, runs a plan and an error path -- no Python or torch in between.
+And the header-only C++ layer (include/fftb.hpp) from tests/cpp_api_example.cpp: plan
+registry, ffts 3D / 4D, the reference's exception types, autotune cache, batches."""
 import os
 import subprocess
 
@@ -24,3 +26,16 @@ def test_c_program_uses_the_abi(tmp_path, torch_cuda):
     print(p.stdout)
     assert p.returncode == 0, p.stdout + p.stderr
     assert p.stdout.strip().endswith("ok")
+
+
+def test_cpp_program_uses_the_header_layer(tmp_path, torch_cuda):
+    from fftm_b200 import build
+    from test_abi import _build_cpp_example
+    lib = build.build()
+    exe = tmp_path / "cpp_api_example"
+    _build_cpp_example(lib, exe)
+    p = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=300)
+    print(p.stdout)
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert p.stdout.strip().endswith("ok")
+    assert "FAIL" not in p.stdout
