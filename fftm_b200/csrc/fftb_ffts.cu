@@ -744,9 +744,14 @@ int fftb_ffts_gradient(fftb_ffts o, const void *in, void *const *outs)
         if (!outs[a]) return FFTB_ERROR_INVALID_VALUE;
     int st = ensure_spectrum(o, &o->dspec);
     if (st == FFTB_SUCCESS) st = ensure_spectrum(o, &o->dspec2);
+    if (st != FFTB_SUCCESS) return st;
+    bool outs_aligned = true;
+    for (int a = 0; a < o->dim; ++a) outs_aligned = outs_aligned && aligned16(in, outs[a]);
+    if (o->fused.enabled && outs_aligned)  // 7 launches: the multiply rides in the column pass
+        return fused3d_gradient(o->fused, in, o->dspec, o->dspec2, outs, o->stream, o->timing ? &o->timer : nullptr);
     // one forward transform; per axis the i k multiply into the second buffer (the
     // backward transform consumes its input) and the backward transform
-    if (st == FFTB_SUCCESS) st = fftb_ffts_forward(o, in, o->dspec);
+    st = fftb_ffts_forward(o, in, o->dspec);
     for (int a = 0; a < o->dim && st == FFTB_SUCCESS; ++a) {
         st = fftb_ffts_spectrum_derivative(o, o->dspec, o->dspec2, a, 1.0 / points(o));
         if (st == FFTB_SUCCESS) st = fftb_ffts_backward(o, o->dspec2, outs[a]);

@@ -449,7 +449,8 @@ __device__ __forceinline__ void xcol_fft(cpx<R> (&v)[16], cpx<R> *scr, const cpx
     }
 }
 
-// MODE 0: forward, 1: inverse, 2: forward -> spectral multiply -> inverse (all in place),
+// MODE 0: forward, 1: inverse, 2: forward -> spectral multiply -> inverse (in place, or
+// into tdata, laid out like data, when tdata is given),
 // 3: forward, written transposed: column col becomes the contiguous row tout[col][kx],
 // 4: inverse of 3: reads the rows tin[col][kx], writes the columns in place of `data`.
 // blockIdx.y selects a batch of column sets `bstride` elements apart (the transposed
@@ -573,8 +574,9 @@ __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data,
             dstp[(size_t)rr * NX + kx] = scr[rr * RP + kx];
         }
     } else if (ok) {
+        C *q = (MODE == 2 && tdata) ? tdata + (size_t)blockIdx.y * bstride + cg0 : p;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) p[(size_t)(t + T * j) * stride] = v[j];
+        for (int j = 0; j < 16; ++j) q[(size_t)(t + T * j) * stride] = v[j];
     }
 }
 
@@ -866,6 +868,33 @@ int fused3d_derivative(const Fused3D &f, const void *in, void *spec, void *out, 
                            t);
     }
     if (st == FFTB_SUCCESS) st = launch_plane(f, true, spec, out, 1.0 / (double)(f.nx * f.ny * f.nz), s, t);
+    if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
+    return st;
+}
+
+// every first derivative: the planes' R2C once into spec; per axis the column sandwich
+// with the i k multiply from spec into spec2 and the inverse planes into outs[axis]
+int fused3d_gradient(const Fused3D &f, const void *in, void *spec, void *spec2, void *const *outs, cudaStream_t s,
+                     LaunchTimer *t)
+{
+    const long long nzh = f.nz / 2 + 1;
+    int st = launch_plane(f, false, in, spec, 1.0, s, t);
+    for (int a = 0; a < 3 && st == FFTB_SUCCESS; ++a) {
+        XColEp x = make_ep(nullptr);
+        x.mode = EP_DERIV;
+        x.daxis = a;
+        x.dscale = 1.0;
+        x.dscale_f = 1.f;
+        x.nzh = (int)nzh;
+        x.ny = (int)f.ny;
+        x.nz = (int)f.nz;
+        x.hn = (int)f.nz;
+        x.tc = f.tc ? 1 : 0;
+        st = launch_xcol_n((const XColEntry *)f.xcol, 2, spec, f.ny * nzh, f.ny * nzh, 1, 0, spec2, f.roots_x, x, s,
+                           t);
+        if (st == FFTB_SUCCESS)
+            st = launch_plane(f, true, spec2, outs[a], 1.0 / (double)(f.nx * f.ny * f.nz), s, t);
+    }
     if (st == FFTB_SUCCESS && t) st = timer_end(t, s);
     return st;
 }

@@ -35,6 +35,9 @@ int fused3d_backward_adjoint(const Fused3D &f, const void *greal, void *gspec, c
 // du/d(axis) (0 = x, 1 = y, 2 = z) through the spectrum buffer spec: 3 launches
 int fused3d_derivative(const Fused3D &f, const void *in, void *spec, void *out, int axis, cudaStream_t s,
                        LaunchTimer *t);
+// all three first derivatives: 7 launches, the spectrum written once and read per axis
+int fused3d_gradient(const Fused3D &f, const void *in, void *spec, void *spec2, void *const *outs, cudaStream_t s,
+                     LaunchTimer *t);
 int fused3d_num_launches(const Fused3D &f, int which);
 
 // 4D slab / native_xzwy with power-of-two (z, w) planes and x, y column kernels.
