@@ -325,15 +325,27 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
                 }
             }
             regfft_warp<R, NY, +1>(v, col, twy, t);
-            // back into the staging column, then push whole row segments to the row owners
-            __syncwarp();
+            if constexpr (CL == 1) {
+                // one CTA per plane: straight from the registers into the rows (row
+                // t + TY j), no staging round trip and one barrier per block
+                if (ok) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) col[t + TY * j] = v[j];
-            __syncthreads();
-            for (int e = tid; e < NY * ns; e += S::NT) {
-                const int m = e / ns, q = e - (e / ns) * ns;
-                const int owner = m / S::M;
-                dst[owner][(m - owner * S::M) * S::PR + c * S::S + s0 + q] = cur[q * S::PC + m];
+                    for (int j = 0; j < 16; ++j) rowsm[(t + TY * j) * S::PR + sl] = v[j];
+                }
+            } else {
+                // back into the staging column, then push whole row segments to the row
+                // owners: contiguous slots per row keep the distributed-shared-memory stores
+                // coalesced (pushing every register straight to its owner scatters them one
+                // row per lane, measured 7% slower at 256x256 with 2-CTA clusters)
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < 16; ++j) col[t + TY * j] = v[j];
+                __syncthreads();
+                for (int e = tid; e < NY * ns; e += S::NT) {
+                    const int m = e / ns, q = e - (e / ns) * ns;
+                    const int owner = m / S::M;
+                    dst[owner][(m - owner * S::M) * S::PR + c * S::S + s0 + q] = cur[q * S::PC + m];
+                }
             }
             __syncthreads();  // the staging area is refilled for the next block
             if (s0 + FY < S::S) stage(s0 + FY, stg);
