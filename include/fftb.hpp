@@ -13,6 +13,7 @@
  *   fftb::load_or_measure_config  load_or_measure_3d_config
  *                              (source/fftm_autotune.hpp:46-70, source/fftm_autotune_measure.hpp:432-520)
  *   fftb::batch<T>             many uneven 3D transforms in one graph-replayed launch
+ *   fftb::poisson3d_noalloc    the allocation-free float32 3D Poisson solve
  *
  * Error behaviour is the reference's: API misuse throws std::logic_error (init twice, not
  * initialised, wrong dimension, plans added after activation -- source/ffts.hpp:631-657,
@@ -631,6 +632,18 @@ private:
     std::array<long long, 4> n_{};
     std::size_t dim_ = 0;
 };
+
+/* The allocation-free 3D float32 Poisson solve (fftb_poisson3d_f32_noalloc): static
+ * device scratch, spectra up to FFTB_NOALLOC_MAX_SPECTRUM_BYTES, overlapping calls
+ * serialised by the caller. */
+template <class In, class Out>
+void poisson3d_noalloc(const In &rhs, Out &u, long long nx, long long ny, long long nz, double sign = -1.0,
+                       cudaStream_t stream = nullptr)
+{
+    check(fftb_poisson3d_f32_noalloc(static_cast<const float *>(detail::raw(rhs)), static_cast<float *>(detail::raw(u)),
+                                     nx, ny, nz, sign, (void *)stream),
+          "poisson3d_noalloc");
+}
 
 /* ====================================================================== batches */
 

@@ -4,7 +4,8 @@
 //   1. fft_wrap_many<double>: named 3D R2C / C2R plans over arrays with raw_ptr(),
 //      a single-mode known answer and a round trip;
 //   2. the reference's error behaviour: logic_error / out_of_range / runtime_error;
-//   3. ffts<float> 3D: Poisson and a derivative against closed-form solutions;
+//   3. ffts<float> 3D: Poisson (and the allocation-free solve) and a derivative against
+//      closed-form solutions;
 //   4. ffts<double, native_xzwy> 4D round trip;
 //   5. load_or_measure_config: measured once, then read back from the cache;
 //   6. batch<float>: uneven 3D round trips in one graph-replayed launch.
@@ -182,6 +183,9 @@ void ffts_3d()
     u_in.put(uf);
     f.derivative(u_in, du, 1);
     expect(rel_l2(du.get(), uy_exact) < 1e-5, "ffts<float>::derivative (y) vs the exact derivative");
+    device_array<float> u_na(n);
+    fftb::poisson3d_noalloc(d_rhs, u_na, N, N, N, -1.0);
+    expect(rel_l2(u_na.get(), u_exact) < 1e-5, "poisson3d_noalloc vs the exact solution");
 }
 
 void ffts_4d_native()
