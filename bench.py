@@ -542,6 +542,23 @@ def main():
         del x4p, y4p, w4p
     except Exception as exc:  # noqa: BLE001
         more["poisson4d_64"] = {"unavailable": str(exc)[:200]}
+    # spectral derivative and gradient of the 256^3 field (the reference test's
+    # derivative_spectra_functor pipeline); algorithmic bytes: one read of u, one write per
+    # derivative
+    try:
+        xd = torch.from_numpy(np.random.default_rng(0).uniform(-1, 1, (NX, NY, NZ)).astype(np.float32)).to(dev)
+        outs = [torch.empty_like(xd) for _ in range(3)]
+        ms = time_events(lambda: ff.derivative(xd, outs[0], 1), 30)
+        t = statistics.median(ms)
+        more["derivative_256"] = {"workload": "du/dy of a 256^3 f32 field, U[-1,1] default_rng(0)",
+                                  "median_us": t * 1e3, "value": 8 * NX * NY * NZ / (t * 1e-3) / 1e9, "unit": "GB/s"}
+        ms = time_events(lambda: ff.gradient(xd, outs), 30)
+        t = statistics.median(ms)
+        more["gradient_256"] = {"workload": "(du/dx, du/dy, du/dz) of a 256^3 f32 field, U[-1,1] default_rng(0)",
+                                "median_us": t * 1e3, "value": 16 * NX * NY * NZ / (t * 1e-3) / 1e9, "unit": "GB/s"}
+        del xd, outs
+    except Exception as exc:  # noqa: BLE001
+        more["derivative_256"] = {"unavailable": str(exc)[:200]}
 
     # batched uneven 3D transforms: 512 shapes with every axis drawn from {32, 48, 64, 96, 128}
     # (numpy default_rng(2)); one step = the R2C + normalised C2R round trip of every transform.
