@@ -2,6 +2,7 @@
 a profiler (``ncu -k ... -s ... -c ...``) sees a short, predictable launch sequence.
 
   python -m fftm_b200.profile_case poisson3d --n 256 --reps 3      # fused 3D Poisson solve
+  python -m fftm_b200.profile_case poisson3d --n 256 --cluster 4   # same, 4-CTA plane clusters
   python -m fftm_b200.profile_case staged3d --n 256 --reps 3       # same, one pass kernel per axis
   python -m fftm_b200.profile_case roundtrip4d --n 64 --reps 3     # 4D R2C + normalised C2R
   python -m fftm_b200.profile_case batch --count 512 --reps 2      # batched round trips
@@ -26,6 +27,8 @@ def main(argv=None) -> int:
     ap.add_argument("--count", type=int, default=512)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--mode", type=int, default=2, help="batch mode: 0 sequential, 1 persistent, 2 graph")
+    ap.add_argument("--cluster", type=int, default=0,
+                    help="poisson3d: CTAs per plane of the fused kernels (1, 2, 4, 8; 0 = the library's choice)")
     a = ap.parse_args(argv)
 
     import torch
@@ -38,6 +41,8 @@ def main(argv=None) -> int:
         f = F.ffts("float32").init(n, n, n)
         if a.case == "staged3d":
             f.set_strategy("staged")
+        elif a.cluster:
+            f.set_strategy("fused", a.cluster)
         x = torch.rand((n, n, n), device=dev, generator=gen) - 0.5
         x -= x.mean()
         y = torch.empty_like(x)
