@@ -10,9 +10,10 @@ Pins used (the reference stores no golden vectors for this path):
     source/tests/detail/versioned_ffts_3d_test_driver.h:186-210);
   * the reference benchmarks' round-trip criterion RMS(C2R(R2C(x))/N - x) <= 10 eps
     (source/tests/test_benchmark_ffts_3D.cu:100-120, fft_benchmark_common.h:28-32);
-  * the reference Poisson test problem, a Gaussian-modulated sine with closed-form
-    solution and gradient (source/tests/detail/poisson_3d_problem.h:22-50), whose L2 and
-    H1 errors the reference reports (source/tests/test_3D_poisson.cu:247-280).
+  * the reference Poisson test problems, Gaussian-modulated sines with closed-form
+    solutions (source/tests/detail/poisson_3d_problem.h:22-50 with its gradient,
+    poisson_4d_problem.h:14-55), whose L2 and H1 errors the reference reports
+    (source/tests/test_3D_poisson.cu:247-280).
 """
 import os
 
@@ -112,6 +113,34 @@ def test_oracle_gaussian_sine_poisson_problem():
         errs.append((O.rel_l2(sol, u), O.rel_l2(dsol, ux)))
     assert errs[0][0] < 1e-4 and errs[1][0] < errs[0][0]
     assert errs[0][1] < 1e-3 and errs[1][1] < errs[0][1]
+
+
+def _gaussian_sine_problem_4d(n):
+    # the 4D problem of the reference (poisson_4d_problem<T>::evaluate,
+    # source/tests/detail/poisson_4d_problem.h:14-55): u = 100 g sin x sin y sin z sin w
+    g1 = _grid(n)
+    x, y, z, w = np.meshgrid(g1, g1, g1, g1, indexing="ij")
+    d = [x - np.pi, y - np.pi, z - np.pi, w - np.pi]
+    s = [np.sin(x), np.sin(y), np.sin(z), np.sin(w)]
+    c = [np.cos(x), np.cos(y), np.cos(z), np.cos(w)]
+    g = np.exp(-sum(a * a for a in d))
+    prod = s[0] * s[1] * s[2] * s[3]
+    f = (4 * sum(a * a for a in d) - 12) * prod
+    for a in range(4):
+        others = np.prod([s[b] for b in range(4) if b != a], axis=0)
+        f = f - 4 * d[a] * c[a] * others
+    return 100 * g * prod, 100 * g * f
+
+
+@pytest.mark.parametrize("layout", [O.PENCIL, O.SLAB, O.NATIVE_XZWY])
+def test_oracle_gaussian_sine_poisson_problem_4d(layout):
+    errs = []
+    for n in (16, 24):
+        u, f = _gaussian_sine_problem_4d(n)
+        if layout == O.PENCIL:   # pencil real arrays are stored [w][z][y][x]
+            u, f = (np.ascontiguousarray(a.transpose(3, 2, 1, 0)) for a in (u, f))
+        errs.append(O.rel_l2(O.poisson4d_solve(layout, f, (n,) * 4, sign=-1.0), u))
+    assert errs[0] < 2e-4 and errs[1] < errs[0], errs
 
 
 @pytest.mark.parametrize("layout", [O.PENCIL, O.SLAB, O.NATIVE_XZWY])
