@@ -73,6 +73,50 @@ template <int N> __device__ __forceinline__ void cp_async_wait_group()
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// L2 eviction policies (createpolicy) and loads / stores that carry them: evict_first for
+// data read or written once (the real fields), evict_last for data the next kernel of the
+// same transform reads again (the spectrum), so the streaming fields do not push it out.
+__device__ __forceinline__ unsigned long long l2_evict_first()
+{
+    unsigned long long p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ unsigned long long l2_evict_last()
+{
+    unsigned long long p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ float ld_hint(const float *g, unsigned long long pol)
+{
+    float v;
+    asm volatile("ld.global.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;\n" : "=f"(v) : "l"(g), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float2 ld_hint(const float2 *g, unsigned long long pol)
+{
+    float2 v;
+    asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;\n"
+                 : "=f"(v.x), "=f"(v.y) : "l"(g), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_hint(float *g, float v, unsigned long long pol)
+{
+    asm volatile("st.global.L1::no_allocate.L2::cache_hint.f32 [%0], %1, %2;\n" ::"l"(g), "f"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_hint(float2 *g, float2 v, unsigned long long pol)
+{
+    asm volatile("st.global.L1::no_allocate.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;\n" ::"l"(g), "f"(v.x), "f"(v.y),
+                 "l"(pol)
+                 : "memory");
+}
+// Asynchronous prefetch of BYTES (a multiple of 16, 16-byte aligned) of global memory into L2.
+__device__ __forceinline__ void prefetch_l2(const void *g, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(g), "r"(bytes) : "memory");
+}
+
 // Shared-memory index padding: one spare slot per 16 entries keeps the
 // stride-R Stockham scatters free of bank conflicts.
 __host__ __device__ constexpr int pad16(int a) { return a + (a >> 4); }

@@ -33,7 +33,7 @@ thread_local std::string g_last_error;
 
 struct Registry {
     std::map<int, PassKernelInfo> tab[2];
-    std::set<const void *> smem_configured;
+    std::set<std::pair<int, const void *>> smem_configured;  // (device, kernel): the limit is per device
     std::map<std::tuple<int, int, int>, void *> roots;  // (device, dtype, ntw) -> device table
     std::mutex mu;
 
@@ -283,10 +283,15 @@ int program_add(Program &prog, int dtype, const AxisPass &p)
     L.grid = dim3((unsigned)ncta, 1, 1);
     {
         std::lock_guard<std::mutex> lk(r.mu);
-        if (L.smem > 48 * 1024 && !r.smem_configured.count(L.k.fn)) {
-            cudaError_t e = cudaFuncSetAttribute(L.k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        if (L.smem > 48 * 1024) {
+            int dev = 0;
+            cudaError_t e = cudaGetDevice(&dev);
             if (e != cudaSuccess) return set_status_from_cuda(e);
-            r.smem_configured.insert(L.k.fn);
+            if (!r.smem_configured.count({dev, L.k.fn})) {
+                e = cudaFuncSetAttribute(L.k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+                if (e != cudaSuccess) return set_status_from_cuda(e);
+                r.smem_configured.insert({dev, L.k.fn});
+            }
         }
     }
     L.in_buf = p.in_buf;

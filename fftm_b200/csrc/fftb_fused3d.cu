@@ -33,6 +33,13 @@ namespace cg = cooperative_groups;
 
 namespace fftb {
 
+// Cluster barrier split into its two halves: every CTA arrives at kernel entry and waits
+// before its first distributed-shared-memory store, which guarantees that every CTA of the
+// cluster has started (its shared memory exists) before any peer writes into it, while the
+// stage-table build overlaps the barrier.
+__device__ __forceinline__ void cluster_arrive_relaxed() { asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory"); }
+
 // ------------------------------------------------------------------ plane kernels
 // Work split (CL CTAs per plane, CL in {1, 2, 4, 8}):
 //   rows   : CTA c owns rows [c*M, (c+1)*M) for the z stage            (M = NY / CL)
@@ -109,6 +116,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
     C *scr = plane + NY * S::PF;
     C *twz = scr + S::SCRF;                       // stage table of the z FFT
     C *twy = twz + NZ;                            // stage table of the y FFT
+    if constexpr (CL > 1) cluster_arrive_relaxed();
     const int tid = threadIdx.x;
     const int c = (CL > 1) ? (int)cg::this_cluster().block_rank() : 0;
     const int x = (int)(blockIdx.x / CL);
@@ -122,6 +130,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
     build_stage_table<R, NZ>(twz, roots, S::NMAX, tid, S::NT);
     build_stage_table<R, NY>(twy, roots, S::NMAX, tid, S::NT);
     __syncthreads();
+    if constexpr (CL > 1) cluster_wait();  // every peer's shared memory exists from here on
 
     // ---- stage z: R2C of this CTA's rows (two rows per complex FFT), pushed to the slot owners
     {
@@ -263,6 +272,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
     C *twz = stg + S::STG;
     C *twy = twz + NZ;
     C *nyq = twy + NY;                            // the kz = NZ/2 column (CTA 0 of a cluster)
+    if constexpr (CL > 1) cluster_arrive_relaxed();
     const int tid = threadIdx.x;
     const int c = (CL > 1) ? (int)cg::this_cluster().block_rank() : 0;
     const int x = (int)(blockIdx.x / CL);
@@ -273,10 +283,11 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
 #pragma unroll
         for (int q = 0; q < CL; ++q) dst[q] = cg::this_cluster().map_shared_rank(rowsm, (unsigned)q);
     }
+    const C *iplane = in + (size_t)x * NY * (NZ / 2 + 1);
     build_stage_table<R, NZ>(twz, roots, S::NMAX, tid, S::NT);
     build_stage_table<R, NY>(twy, roots, S::NMAX, tid, S::NT);
     __syncthreads();
-    const C *iplane = in + (size_t)x * NY * (NZ / 2 + 1);
+    if constexpr (CL > 1) cluster_wait();  // every peer's shared memory exists from here on
 
     // ---- stage y: inverse FFT of the owned slots, rows pushed to their owners
     {

@@ -93,9 +93,15 @@ struct NaPass {
 int launch_pass(const NaPass &p, cudaStream_t stream)
 {
     const bool realk = (p.kind == K_R2C || p.kind == K_C2R);
-    const bool half = realk && (p.n % 2 == 0);
-    const int nf = half ? p.n / 2 : p.n;
+    bool half = realk && (p.n % 2 == 0);
+    int nf = half ? p.n / 2 : p.n;
     PassKernelInfo k;
+    if (half && !lookup_kernel(FFTB_F32, nf, &k)) {
+        // no half-length kernel: the real line runs as a full complex line of length n,
+        // as the regular pass programs do (its root table, [0], has length n)
+        half = false;
+        nf = p.n;
+    }
     if (!lookup_kernel(FFTB_F32, nf, &k)) return FFTB_ERROR_UNSUPPORTED_SIZE;
     PassArgs a;
     memset(&a, 0, sizeof(a));
@@ -168,10 +174,14 @@ extern "C" int fftb_poisson3d_f32_noalloc(const float *rhs, float *solution, lon
         set_last_error("spectrum larger than the static scratch of fftb_poisson3d_f32_noalloc");
         return FFTB_ERROR_INVALID_VALUE;
     }
-    // every line length must have a pass kernel (R2C/C2R of even nz run nz/2)
-    const int nfz = (nz % 2 == 0) ? (int)(nz / 2) : (int)nz;
-    if (!has_kernel(FFTB_F32, nfz) || !has_kernel(FFTB_F32, (int)ny) || !has_kernel(FFTB_F32, (int)nx))
+    // every line length must have a pass kernel of its own (R2C/C2R of even nz run nz/2, or
+    // nz as a full complex line when nz/2 has none); lengths that need the chirp-z passes do
+    // not, since those need a padded work line of their own
+    const bool zok = has_kernel(FFTB_F32, (int)nz) || (nz % 2 == 0 && has_kernel(FFTB_F32, (int)(nz / 2)));
+    if (!zok || !has_kernel(FFTB_F32, (int)ny) || !has_kernel(FFTB_F32, (int)nx)) {
+        set_last_error("fftb_poisson3d_f32_noalloc: a line length has no direct pass kernel");
         return FFTB_ERROR_UNSUPPORTED_SIZE;
+    }
     if ((uintptr_t)rhs % sizeof(float) || (uintptr_t)solution % sizeof(float)) return FFTB_ERROR_MISALIGNED;
     void *base = nullptr;
     int st = scratch_address(&base);

@@ -311,9 +311,13 @@ int fftb_batch_apply_config(fftb_batch batch, const char *text, int *mode);
  * Same result as fftb_ffts_poisson on a float32 [x][y][z] field: u = C2R(sign *
  * R2C(f) / |k|^2) / N with k = 0 set to 0.  rhs and solution are caller-owned
  * device arrays of nx*ny*nz floats (they may alias); stream is a cudaStream_t
- * (NULL: the legacy default stream).  2 <= nx, ny, nz <= 4096, every length a
- * supported line length, and the spectrum at most FFTB_NOALLOC_MAX_SPECTRUM_BYTES
- * (e.g. 128^3); larger sizes return FFTB_ERROR_INVALID_VALUE.
+ * (NULL: the legacy default stream).  2 <= nx, ny, nz <= 4096 and the spectrum at
+ * most FFTB_NOALLOC_MAX_SPECTRUM_BYTES (e.g. 128^3); larger sizes return
+ * FFTB_ERROR_INVALID_VALUE.  Every line length must have a direct pass kernel (the
+ * lengths 2^a * {1, 3, 5, 7, 9, 15, 21, 25, 27}, 11 and 13 times a power of two up to
+ * 832, and the odd products listed with the pass kernels; for nz, nz or nz/2): lengths
+ * that the regular path runs through chirp-z passes (a large prime factor) need a padded
+ * work line and return FFTB_ERROR_UNSUPPORTED_SIZE here.
  *
  * The scratch (twiddle tables and spectrum) is one static __device__ array that
  * every GPU loading the library holds until the process exits.  The first call on

@@ -2,10 +2,12 @@
 device memory (for callers that cannot call cudaMalloc, e.g. when a framework's
 memory pool owns the device).
 
-It is called through the C ABI twice in a row, with different fields and sizes,
-and each result is compared with the regular entry point (fftb_ffts_poisson via
-the ffts object) at the float32 tolerance of the other GPU tests (relative L2
-2e-6).  The file is named so that pytest collects it last.
+It is called through the C ABI twice in a row over a set of fields and sizes (mixed
+sizes, a power-of-two cube that the regular entry point runs through its fused plane
+and column kernels, and an odd z length whose R2C/C2R run full complex lines), and each
+result is compared with the FP64 oracle and with the regular entry point
+(fftb_ffts_poisson via the ffts object) at the float32 tolerance of the other GPU tests
+(relative L2 2e-6).  The file is named so that pytest collects it last.
 """
 import ctypes
 
@@ -50,7 +52,8 @@ def _regular(torch, rhs, sign):
 
 def test_noalloc_matches_regular_entry_point_on_two_calls(lib, torch_cuda):
     torch = torch_cuda
-    cases = [((32, 24, 16), 11, -1.0), ((64, 48, 40), 12, 1.0)]
+    cases = [((32, 24, 16), 11, -1.0), ((64, 48, 40), 12, 1.0), ((64, 64, 64), 13, -1.0),
+             ((16, 12, 15), 14, -1.0)]
     rhs = [torch.tensor(O.random_3d(*shape, seed, single=True), dtype=torch.float32, device="cuda")
            for shape, seed, _ in cases]
     sol = [torch.empty_like(r) for r in rhs]
@@ -68,9 +71,13 @@ def test_noalloc_matches_regular_entry_point_on_two_calls(lib, torch_cuda):
     torch.cuda.synchronize()
     assert torch.cuda.mem_get_info()[0] == free_before      # the two calls allocated nothing
     for (shape, seed, sign), r, s in zip(cases, rhs, sol):
+        got = s.cpu().numpy().astype(np.float64)
+        exact = O.poisson3d_solve(r.cpu().numpy().astype(np.float64), sign)
+        err = O.rel_l2(got, exact)
+        assert err <= TOL, (shape, "vs FP64 oracle", err)
         ref = _regular(torch, r, sign)
-        err = O.rel_l2(s.cpu().numpy().astype(np.float64), ref.cpu().numpy().astype(np.float64))
-        assert err <= TOL, (shape, err)
+        err = O.rel_l2(got, ref.cpu().numpy().astype(np.float64))
+        assert err <= TOL, (shape, "vs fftb_ffts_poisson", err)
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(lib, torch_cuda):
