@@ -117,6 +117,61 @@ __device__ __forceinline__ void prefetch_l2(const void *g, unsigned bytes)
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(g), "r"(bytes) : "memory");
 }
 
+// ---------------------------------------------------------------- bulk copies (TMA)
+// mbarrier-tracked tensor copies global -> shared (no multicast: every copy reads this
+// GPU's own memory into this CTA's shared memory).
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// makes initialised barriers visible to the asynchronous (copy) proxy
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// Bounded wait for the phase with the given parity: false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, int limit)
+{
+    for (int i = 0; i < limit; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (i >= 16) __nanosleep(128);
+    }
+    return false;
+}
+// Orders this thread's generic-proxy shared-memory accesses before later bulk copies.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// 3D tiled tensor copy into this CTA's shared memory, completing on `bar` (byte count).
+// The innermost coordinate x times the element size must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, unsigned long long *bar, int x, int y, int z)
+{
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%3, %4, %5}], [%2];\n" ::"r"(smem_u32(dst)),
+                 "l"(tmap), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+
+// Approximate reciprocal (one MUFU operation, relative error at most 2^-23 per the PTX
+// specification of rcp.approx.f32): for factors whose rounding error is far below the
+// transforms' own.
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;\n" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // Shared-memory index padding: one spare slot per 16 entries keeps the
 // stride-R Stockham scatters free of bank conflicts.
 __host__ __device__ constexpr int pad16(int a) { return a + (a >> 4); }

@@ -19,8 +19,11 @@
 // shared memory with distributed-shared-memory stores, so no plane round-trips
 // through global memory between the z and y stages.
 #include <cooperative_groups.h>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstdint>
 #include <cstdlib>
 #include <string>
 
@@ -62,7 +65,6 @@ template <int NY, int NZ, int CL, int NT_> struct PlaneShapeT {
     static constexpr int TY = RegFFTShape<NY>::T;
     static constexpr int FZ = NT / TZ, FY = NT / TY;         // concurrent FFTs per stage
     static constexpr int NMAX = NY > NZ ? NY : NZ;
-    static constexpr int TWS = NY + NZ;                      // stage tables of the z and y FFTs
     // forward: y-stage plane [NY][PF], PF = 16/TY (mod 16) -> conflict-free column reads
     static constexpr int PMOD = 16 / TY;
     static constexpr int PF = S + ((PMOD - S % 16) % 16 + 16) % 16;
@@ -78,11 +80,11 @@ template <int NY, int NZ, int CL, int NT_> struct PlaneShapeT {
     static constexpr int STG = FY * PC > SCR_Z ? FY * PC : SCR_Z;
     template <typename R> static constexpr size_t smem_fwd()
     {
-        return sizeof(cpx<R>) * ((size_t)NY * PF + SCRF + TWS);
+        return sizeof(cpx<R>) * ((size_t)NY * PF + SCRF);
     }
     template <typename R> static constexpr size_t smem_inv()
     {
-        return sizeof(cpx<R>) * ((size_t)M * PR + STG + TWS + NY);  // + the staged kz = NZ/2 column
+        return sizeof(cpx<R>) * ((size_t)M * PR + STG + NY);  // + the staged kz = NZ/2 column
     }
     // CTAs per SM the register budget is sized for: 8-CTA clusters keep a CTA's shared
     // memory under a third of the SM's, so three CTAs (24 warps) fit when registers are
@@ -114,8 +116,6 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *plane = reinterpret_cast<C *>(smem_raw);   // [NY][PF]: this CTA's column slots
     C *scr = plane + NY * S::PF;
-    C *twz = scr + S::SCRF;                       // stage table of the z FFT
-    C *twy = twz + NZ;                            // stage table of the y FFT
     if constexpr (CL > 1) cluster_arrive_relaxed();
     const int tid = threadIdx.x;
     const int c = (CL > 1) ? (int)cg::this_cluster().block_rank() : 0;
@@ -127,15 +127,14 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
 #pragma unroll
         for (int q = 0; q < CL; ++q) dst[q] = cg::this_cluster().map_shared_rank(plane, (unsigned)q);
     }
-    build_stage_table<R, NZ>(twz, roots, S::NMAX, tid, S::NT);
-    build_stage_table<R, NY>(twy, roots, S::NMAX, tid, S::NT);
-    __syncthreads();
     if constexpr (CL > 1) cluster_wait();  // every peer's shared memory exists from here on
 
     // ---- stage z: R2C of this CTA's rows (two rows per complex FFT), pushed to the slot owners
     {
         constexpr int TZ = S::TZ, FZ = S::FZ;
         const int f = tid / TZ, t = tid - (tid / TZ) * TZ;
+        C twz[16];
+        load_stage_twiddles<R, NZ>(twz, roots, S::NMAX, t);
         C *reg = scr + f * RegFFTShape<NZ>::REGION;
         const R *rows = in + ((size_t)x * NY + (size_t)c * S::M) * NZ;
         // the rows of the next round are loaded into registers before this round's FFT,
@@ -168,7 +167,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
             } else {
                 load_rows(p0, v);
             }
-            regfft_warp<R, NZ, -1>(v, reg, twz, t);
+            regfft_warp_rt<R, NZ, -1>(v, reg, twz, t);
             // separate the two real rows with Z[-k] fetched from the partner lane:
             // Z[t + TZ j] sits in lane t, register j; Z[NZ - (t + TZ j)] in lane (TZ - t) mod TZ,
             // register 15 - j (t > 0) or in this lane, register (16 - j) mod 16 (t = 0)
@@ -211,6 +210,8 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
     {
         constexpr int TY = S::TY, FY = S::FY;
         const int f = tid / TY, t = tid - (tid / TY) * TY;
+        C twy[16];
+        load_stage_twiddles<R, NY>(twy, roots, S::NMAX, t);
         C *reg = scr + f * RegFFTShape<NY>::REGION;
         C *oplane = out + (size_t)x * NY * (NZ / 2 + 1);
 #pragma unroll 1
@@ -221,7 +222,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
             C v[16];
 #pragma unroll
             for (int r = 0; r < 16; ++r) v[r] = plane[(t + TY * r) * S::PF + slc];
-            regfft_warp<R, NY, -1>(v, reg, twy, t);
+            regfft_warp_rt<R, NY, -1>(v, reg, twy, t);
             // the packed slot (slot 0 of CTA 0, first round, warp 0):
             // X0[ky] = (W[ky] + conj W[-ky]) / 2, XN[ky] = (W[ky] - conj W[-ky]) / 2i
             if (c == 0 && s0 == 0 && (tid >> 5) == 0) {
@@ -269,9 +270,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *rowsm = reinterpret_cast<C *>(smem_raw);   // [M][PR]: this CTA's rows, every slot
     C *stg = rowsm + S::M * S::PR;                // column staging / FFT exchange regions
-    C *twz = stg + S::STG;
-    C *twy = twz + NZ;
-    C *nyq = twy + NY;                            // the kz = NZ/2 column (CTA 0 of a cluster)
+    C *nyq = stg + S::STG;                        // the kz = NZ/2 column (CTA 0 of a cluster)
     if constexpr (CL > 1) cluster_arrive_relaxed();
     const int tid = threadIdx.x;
     const int c = (CL > 1) ? (int)cg::this_cluster().block_rank() : 0;
@@ -284,15 +283,14 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
         for (int q = 0; q < CL; ++q) dst[q] = cg::this_cluster().map_shared_rank(rowsm, (unsigned)q);
     }
     const C *iplane = in + (size_t)x * NY * (NZ / 2 + 1);
-    build_stage_table<R, NZ>(twz, roots, S::NMAX, tid, S::NT);
-    build_stage_table<R, NY>(twy, roots, S::NMAX, tid, S::NT);
-    __syncthreads();
     if constexpr (CL > 1) cluster_wait();  // every peer's shared memory exists from here on
 
     // ---- stage y: inverse FFT of the owned slots, rows pushed to their owners
     {
         constexpr int TY = S::TY, FY = S::FY;
         const int f = tid / TY, t = tid - (tid / TY) * TY;
+        C twy[16];
+        load_stage_twiddles<R, NY>(twy, roots, S::NMAX, t);
         // stage the ns columns of block s0 (all NY rows) with coalesced asynchronous copies
         auto stage = [&](int s0, C *buf) {
             const int ns = S::S % FY == 0 ? FY : ((S::S - s0) < FY ? (S::S - s0) : FY);
@@ -335,7 +333,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
                     v[r] = mk<R>(h0.x - hn.y, h0.y + hn.x);
                 }
             }
-            regfft_warp<R, NY, +1>(v, col, twy, t);
+            regfft_warp_rt<R, NY, +1>(v, col, twy, t);
             if constexpr (CL == 1) {
                 // one CTA per plane: straight from the registers into the rows (row
                 // t + TY j), no staging round trip and one barrier per block
@@ -369,6 +367,8 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
     {
         constexpr int TZ = S::TZ, FZ = S::FZ;
         const int f = tid / TZ, t = tid - (tid / TZ) * TZ;
+        C twz[16];
+        load_stage_twiddles<R, NZ>(twz, roots, S::NMAX, t);
         C *reg = stg + f * RegFFTShape<NZ>::REGION;
         R *rows = out + ((size_t)x * NY + (size_t)c * S::M) * NZ;
 #pragma unroll 1
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
                 }
                 v[r] = mk<R>(ha.x - hb.y, ha.y + hb.x);  // Ha + i Hb
             }
-            regfft_warp<R, NZ, +1>(v, reg, twz, t);
+            regfft_warp_rt<R, NZ, +1>(v, reg, twz, t);
             if (ok) {
                 R *ra = rows + (size_t)(2 * pp) * NZ;
                 R *rb = ra + NZ;
@@ -472,6 +472,83 @@ __device__ __forceinline__ void xcol_fft(cpx<R> (&v)[16], cpx<R> *scr, const cpx
     }
 }
 
+// The spectral multiply of the column sandwich (MODE 2): v holds rows kx = t + T*j of column
+// cg0; ky, kz (and kw in 4D) follow from the column index.
+template <typename R, int NX>
+__device__ __forceinline__ void xcol_multiply(cpx<R> (&v)[16], int t, int cg0, const XColEp &ep)
+{
+    constexpr int T = XColShape<NX>::T;
+    // wavenumbers: kx = t + T*j (output row); ky, kz, kw from the column
+    int ky_i, kz, kw = 0;
+    if (ep.nd4) {
+        const int cc = cg0 % (ep.nz * ep.nwh);
+        ky_i = cg0 / (ep.nz * ep.nwh);
+        const int kz_i = cc / ep.nwh;
+        kw = cc - kz_i * ep.nwh;
+        kz = kz_i <= ep.nz / 2 ? kz_i : kz_i - ep.nz;
+    } else {
+        ky_i = cg0 / ep.nzh;
+        kz = cg0 - (cg0 / ep.nzh) * ep.nzh;
+    }
+    const int ky = ky_i <= ep.ny / 2 ? ky_i : ky_i - ep.ny;
+    const R kyz = R(ky * ky + kz * kz + kw * kw);
+    const R sc = sizeof(R) == 4 ? R(ep.scale_f) : R(ep.scale);
+    const R sg = sizeof(R) == 4 ? R(ep.sign_f) : R(ep.sign);
+    if (ep.mode & EP_DERIV) {
+        // i k v * scale with k = kx (row), ky or kz (the column); 3D only.  kz is the half
+        // axis: its Nyquist bin carries the real cosine part, whose derivative the C2R
+        // drops with the imaginary part, the same as a separate multiply does
+        const R ds = sizeof(R) == 4 ? R(ep.dscale_f) : R(ep.dscale);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int kxi = t + T * j;
+            const int k = ep.daxis == 0 ? (kxi <= NX / 2 ? kxi : kxi - NX) : (ep.daxis == 1 ? ky : kz);
+            const R fct = R(k) * ds;
+            v[j] = mk<R>(-fct * v[j].y, fct * v[j].x);
+        }
+    } else if ((ep.mode & (EP_POISSON | EP_GAUSS)) == EP_POISSON) {
+        const R ss = sc * sg;
+        const R tr = R(t);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            // kx = t + T j, or t + T j - NX past the Nyquist row (T j = NX/2 is the Nyquist row
+            // itself only for t = 0); the offsets are compile-time constants
+            R kx;
+            if (T * j < NX / 2) kx = tr + R(T * j);
+            else if (T * j > NX / 2) kx = tr + R(T * j - NX);
+            else kx = t == 0 ? R(NX / 2) : tr + R(T * j - NX);
+            const R k2 = kx * kx + kyz;
+            R fct;
+            if constexpr (sizeof(R) == 4) fct = ss * rcp_approx(k2);  // relative error below 2^-22
+            else fct = ss / k2;
+            if (j == 0 && k2 == R(0)) fct = R(0);  // only row kx = 0 can hold the zero mode
+            v[j] = cscale(v[j], fct);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int kxi = t + T * j;
+            const int kx = kxi <= NX / 2 ? kxi : kxi - NX;
+            const R k2 = R(kx * kx) + kyz;
+            R fct = sc;
+            if (ep.mode & EP_POISSON) fct = (k2 == R(0)) ? R(0) : fct * sg / k2;
+            if (ep.mode & EP_GAUSS) fct *= exp(-k2 * (sizeof(R) == 4 ? R(ep.gauss_f) : R(ep.gauss)));
+            v[j] = cscale(v[j], fct);
+        }
+    }
+}
+
+// EP_HALFW: interior bins of the half axis times hw (the adjoint weights)
+template <typename R> __device__ __forceinline__ void xcol_halfw(cpx<R> (&v)[16], int cg0, const XColEp &ep)
+{
+    const int ih = cg0 % (ep.hn / 2 + 1);
+    if (ih != 0 && 2 * ih != ep.hn) {
+        const R w = sizeof(R) == 4 ? R(ep.hw_f) : R(ep.hw);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = cscale(v[j], w);
+    }
+}
+
 // MODE 0: forward, 1: inverse, 2: forward -> spectral multiply -> inverse (in place, or
 // into tdata, laid out like data, when tdata is given),
 // 3: forward, written transposed: column col becomes the contiguous row tout[col][kx],
@@ -522,68 +599,10 @@ __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data,
     if (MODE == 1 || MODE == 4) xcol_fft<R, NX, +1, TC>(v, scr, tw, t, col, stage, F);
     else xcol_fft<R, NX, -1, TC>(v, scr, tw, t, col, stage, F);
     if (MODE == 2) {
-        // wavenumbers: kx = t + T*j (output row); ky, kz, kw from the column
-        int ky_i, kz, kw = 0;
-        if (ep.nd4) {
-            const int cc = cg0 % (ep.nz * ep.nwh);
-            ky_i = cg0 / (ep.nz * ep.nwh);
-            const int kz_i = cc / ep.nwh;
-            kw = cc - kz_i * ep.nwh;
-            kz = kz_i <= ep.nz / 2 ? kz_i : kz_i - ep.nz;
-        } else {
-            ky_i = cg0 / ep.nzh;
-            kz = cg0 - (cg0 / ep.nzh) * ep.nzh;
-        }
-        const int ky = ky_i <= ep.ny / 2 ? ky_i : ky_i - ep.ny;
-        const R kyz = R(ky * ky + kz * kz + kw * kw);
-        const R sc = sizeof(R) == 4 ? R(ep.scale_f) : R(ep.scale);
-        const R sg = sizeof(R) == 4 ? R(ep.sign_f) : R(ep.sign);
-        if (ep.mode & EP_DERIV) {
-            // i k v * scale with k = kx (row), ky or kz (the column); 3D only.  kz is the half
-            // axis: its Nyquist bin carries the real cosine part, whose derivative the C2R
-            // drops with the imaginary part, the same as a separate multiply does
-            const R ds = sizeof(R) == 4 ? R(ep.dscale_f) : R(ep.dscale);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int kxi = t + T * j;
-                const int k = ep.daxis == 0 ? (kxi <= NX / 2 ? kxi : kxi - NX) : (ep.daxis == 1 ? ky : kz);
-                const R fct = R(k) * ds;
-                v[j] = mk<R>(-fct * v[j].y, fct * v[j].x);
-            }
-        } else if ((ep.mode & (EP_POISSON | EP_GAUSS)) == EP_POISSON) {
-            const R ss = sc * sg;
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int kxi = t + T * j;
-                const int kx = kxi <= NX / 2 ? kxi : kxi - NX;
-                const R k2 = R(kx * kx) + kyz;
-                R inv;
-                if constexpr (sizeof(R) == 4) inv = __frcp_rn(k2);
-                else inv = R(1) / k2;
-                v[j] = cscale(v[j], (k2 == R(0)) ? R(0) : ss * inv);
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int kxi = t + T * j;
-                const int kx = kxi <= NX / 2 ? kxi : kxi - NX;
-                const R k2 = R(kx * kx) + kyz;
-                R fct = sc;
-                if (ep.mode & EP_POISSON) fct = (k2 == R(0)) ? R(0) : fct * sg / k2;
-                if (ep.mode & EP_GAUSS) fct *= exp(-k2 * (sizeof(R) == 4 ? R(ep.gauss_f) : R(ep.gauss)));
-                v[j] = cscale(v[j], fct);
-            }
-        }
+        xcol_multiply<R, NX>(v, t, cg0, ep);
         xcol_fft<R, NX, +1, TC>(v, scr, tw, t, col, stage, F);
     }
-    if (MODE != 2 && (ep.mode & EP_HALFW)) {
-        const int ih = cg0 % (ep.hn / 2 + 1);
-        if (ih != 0 && 2 * ih != ep.hn) {
-            const R w = sizeof(R) == 4 ? R(ep.hw_f) : R(ep.hw);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) v[j] = cscale(v[j], w);
-        }
-    }
+    if (MODE != 2 && (ep.mode & EP_HALFW)) xcol_halfw<R>(v, cg0, ep);
     if (MODE == 3) {
         // columns in registers -> shared memory -> contiguous rows of the transposed output
         __syncthreads();
@@ -600,6 +619,132 @@ __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data,
         C *q = (MODE == 2 && tdata) ? tdata + (size_t)blockIdx.y * bstride + cg0 : p;
 #pragma unroll
         for (int j = 0; j < 16; ++j) q[(size_t)(t + T * j) * stride] = v[j];
+    }
+}
+
+// ------------------------------------------------------------------ x column kernel, TMA ring
+// Persistent form of xcol_kernel (MODE 0, 1, 2) for 16-byte aligned spectra: each CTA walks
+// the tiles (W columns x NX rows; blockIdx.x, + gridDim.x, ...) with NSTAGE tiles in flight,
+// brought into shared memory by tensor copies that one thread issues while the CTA
+// transforms the oldest tile.  A tile's shared memory doubles as the exchange area of its
+// FFTs, so the ring is the only shared memory the kernel needs; each thread keeps its
+// stage twiddles w_NX^(t k1) in registers for every tile it transforms.
+constexpr int kRingStages = 3;
+constexpr int kRingWaitLimit = 1 << 22;  // polls of a bounded bulk-copy wait (seconds)
+__device__ int g_ring_wait_error;        // set when a bounded wait gave up (a copy never completed)
+
+template <typename R, int NX>
+__device__ __forceinline__ void xcol_fft_regtw(cpx<R> (&v)[16], cpx<R> *scr, const cpx<R> (&tw)[16], int t, int col,
+                                               bool inverse)
+{
+    using C = cpx<R>;
+    constexpr int T = XColShape<NX>::T, W = XColShape<NX>::W;
+    if (inverse) dft16<+1, C, R>(v);
+    else dft16<-1, C, R>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < 16; ++k1) v[k1] = inverse ? cmulc(v[k1], tw[k1]) : cmul(v[k1], tw[k1]);
+    __syncthreads();
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) scr[(k1 * T + t) * W + col] = v[k1];
+    __syncthreads();
+    constexpr int A = 16 / T;
+#pragma unroll
+    for (int a = 0; a < A; ++a) {
+        C u[T];
+#pragma unroll
+        for (int q = 0; q < T; ++q) u[q] = scr[((t + T * a) * T + q) * W + col];
+        if (inverse) dft_small<+1, T, C, R>(u);
+        else dft_small<-1, T, C, R>(u);
+#pragma unroll
+        for (int k2 = 0; k2 < T; ++k2) v[a + A * k2] = u[k2];
+    }
+}
+
+// tmap: float32 view [nbatch][NX][2 * ncols] of the spectrum (row pitch `stride`, batch pitch
+// `bstride` complex entries), box {2W, NX, 1}.  Tile k = (batch k / tpb, column block k % tpb).
+template <typename R, int NX, int MODE>
+__global__ void __launch_bounds__(256, 2)
+    xcol_ring_kernel(const __grid_constant__ CUtensorMap tmap, cpx<R> *__restrict__ data, long long stride,
+                     int ncols, int tpb, int ntiles, long long bstride, cpx<R> *__restrict__ tdata,
+                     const cpx<R> *__restrict__ roots, XColEp ep)
+{
+    using C = cpx<R>;
+    constexpr int T = XColShape<NX>::T, W = XColShape<NX>::W;
+    constexpr int TILE = NX * W;
+    constexpr unsigned TILE_BYTES = TILE * sizeof(C);
+    static_assert(16 * T * W <= TILE, "a tile holds its exchange area");
+    // dynamic shared memory: [pad to 128 B][kRingStages tiles][kRingStages mbarriers][flag]; the
+    // tensor copies need 128-byte aligned destinations, so the ring is aligned by hand
+    extern __shared__ __align__(128) unsigned char ring_smem_raw[];
+    const unsigned pad = (128u - (smem_u32(ring_smem_raw) & 127u)) & 127u;
+    C *ring = reinterpret_cast<C *>(ring_smem_raw + pad);
+    unsigned long long *full = reinterpret_cast<unsigned long long *>(ring_smem_raw + pad + kRingStages * TILE_BYTES);
+    int &ok_s = *reinterpret_cast<int *>(full + kRingStages);
+    const int tid = threadIdx.x;
+    const int t = tid / W, col = tid - (tid / W) * W;
+    if ((smem_u32(ring) & 127u) != 0u) {  // never issue a copy to a misaligned destination
+        if (tid == 0) atomicExch(&g_ring_wait_error, 2);
+        return;
+    }
+    auto issue = [&](int stage, int k) {
+        const int b = k / tpb, tx = k - (k / tpb) * tpb;
+        mbar_arrive_expect_tx(&full[stage], TILE_BYTES);
+        tma_load_3d(ring + stage * TILE, &tmap, &full[stage], 2 * W * tx, 0, b);
+    };
+    if (tid == 0) {
+        for (int q = 0; q < kRingStages; ++q) mbar_init(&full[q], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int q = 0; q < kRingStages; ++q)
+            if (blockIdx.x + q * gridDim.x < (unsigned)ntiles) issue(q, blockIdx.x + q * gridDim.x);
+    C tw[16];
+    tw[0] = mk<R>(R(1), R(0));
+#pragma unroll
+    for (int k1 = 1; k1 < 16; ++k1) tw[k1] = roots[t * k1];
+    int it = 0;
+#pragma unroll 1
+    for (int k = blockIdx.x; k < ntiles; k += gridDim.x, ++it) {
+        const int stage = it % kRingStages;
+        if (tid == 0) ok_s = mbar_wait(&full[stage], (unsigned)(it / kRingStages) & 1u, kRingWaitLimit) ? 1 : 0;
+        __syncthreads();
+        if (!ok_s) {
+            // a copy never completed: wait (bounded) for the other copies in flight into this
+            // CTA's shared memory, flag the error and leave
+            if (tid == 0) {
+                for (int q = 1; q < kRingStages; ++q) {
+                    const int kk = k + q * (int)gridDim.x;
+                    if (kk < ntiles) mbar_wait(&full[(it + q) % kRingStages], (unsigned)((it + q) / kRingStages) & 1u,
+                                               kRingWaitLimit);
+                }
+                atomicExch(&g_ring_wait_error, 1);
+            }
+            return;
+        }
+        C *buf = ring + stage * TILE;
+        const int b = k / tpb, tx = k - (k / tpb) * tpb;
+        const int cg0 = tx * W + col;
+        C v[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) v[r] = buf[(t + T * r) * W + col];
+        xcol_fft_regtw<R, NX>(v, buf, tw, t, col, MODE == 1);
+        if (MODE == 2) {
+            xcol_multiply<R, NX>(v, t, cg0, ep);
+            xcol_fft_regtw<R, NX>(v, buf, tw, t, col, true);
+        }
+        if (MODE != 2 && (ep.mode & EP_HALFW)) xcol_halfw<R>(v, cg0, ep);
+        if (cg0 < ncols) {
+            C *q = ((MODE == 2 && tdata) ? tdata : data) + (size_t)b * bstride + cg0;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) q[(size_t)(t + T * j) * stride] = v[j];
+        }
+        __syncthreads();  // every thread is done with this tile's shared memory
+        const int kn = k + kRingStages * (int)gridDim.x;
+        if (tid == 0 && kn < ntiles) {
+            fence_proxy_async_smem();
+            issue(stage, kn);
+        }
     }
 }
 
@@ -642,6 +787,8 @@ struct XColEntry {
     size_t smem;
     const void *fn_tc[5];  // first radix-16 stage on the tensor cores
     size_t smem_tc;
+    const void *fn_ring[3];  // persistent TMA-ring form of modes 0, 1, 2
+    size_t smem_ring;
 };
 
 template <typename R, int NX> XColEntry xcol_entry(int dtype)
@@ -658,7 +805,10 @@ template <typename R, int NX> XColEntry xcol_entry(int dtype)
                      {(const void *)&xcol_kernel<R, NX, 0, true>, (const void *)&xcol_kernel<R, NX, 1, true>,
                       (const void *)&xcol_kernel<R, NX, 2, true>, (const void *)&xcol_kernel<R, NX, 3, true>,
                       (const void *)&xcol_kernel<R, NX, 4, true>},
-                     smem + (size_t)(256 / 32) * kTcWarpBytes};
+                     smem + (size_t)(256 / 32) * kTcWarpBytes,
+                     {(const void *)&xcol_ring_kernel<R, NX, 0>, (const void *)&xcol_ring_kernel<R, NX, 1>,
+                      (const void *)&xcol_ring_kernel<R, NX, 2>},
+                     (size_t)kRingStages * NX * W * sizeof(cpx<R>) + 128 + 64};
 }
 
 const XColEntry *find_xcol(int dtype, int nx)
@@ -755,17 +905,70 @@ XColEp make_ep(const EpValues *ep)
     return x;
 }
 
+int device_sms()
+{
+    static int sms[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!sms[dev] && cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        sms[dev] = 148;
+    return sms[dev];
+}
+
+// The persistent TMA-ring column kernel takes modes 0-2 of a 16-byte aligned spectrum whose
+// row and batch pitches are multiples of 16 bytes (the tensor map's stride rule).
+bool ring_eligible(int mode, const void *data, long long stride, long long nbatch, long long bstride,
+                   const void *tdata, const XColEp &x)
+{
+    if (mode > 2 || x.tc || getenv("FFTB_DISABLE_RING")) return false;
+    if ((uintptr_t)data % 16 || (tdata && (uintptr_t)tdata % 16)) return false;
+    if ((stride * 8) % 16 || (nbatch > 1 && (bstride * 8) % 16)) return false;
+    return true;
+}
+
+int launch_xcol_ring(const XColEntry *e, int mode, void *data, long long stride, long long ncols, long long nbatch,
+                     long long bstride, void *tdata, void *roots, XColEp x, cudaStream_t s)
+{
+    const int W = 256 / (e->nx / 16);
+    CUtensorMap map;
+    const cuuint64_t dims[3] = {(cuuint64_t)(2 * ncols), (cuuint64_t)e->nx, (cuuint64_t)nbatch};
+    const cuuint64_t strides[2] = {(cuuint64_t)(stride * 8),
+                                   (cuuint64_t)((nbatch > 1 ? bstride : stride * e->nx) * 8)};
+    const cuuint32_t box[3] = {(cuuint32_t)(2 * W), (cuuint32_t)e->nx, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = cuTensorMapEncodeTiled(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, data, dims, strides, box, estr,
+                                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_last_error("cuTensorMapEncodeTiled failed for the column kernel's tensor map");
+        return FFTB_ERROR_CUDA;
+    }
+    const long long tpb = (ncols + W - 1) / W, ntiles = tpb * nbatch;
+    const long long ctas = std::min<long long>(ntiles, 2LL * device_sms());
+    float2 *d = (float2 *)data;
+    float2 *td = (float2 *)tdata;
+    int nc = (int)ncols, tp = (int)tpb, nt = (int)ntiles;
+    const float2 *rt = (const float2 *)roots;
+    void *args[] = {&map, &d, &stride, &nc, &tp, &nt, &bstride, &td, &rt, &x};
+    return set_status_from_cuda(
+        cudaLaunchKernel(e->fn_ring[mode], dim3((unsigned)ctas), dim3(256), args, e->smem_ring, s));
+}
+
 // One launch of a column kernel: ncols columns `stride` apart per batch, nbatch batches.
 int launch_xcol_n(const XColEntry *e, int mode, void *data, long long stride, long long ncols, long long nbatch,
                   long long bstride, void *tdata, void *roots, XColEp x, cudaStream_t s, LaunchTimer *tm)
 {
     const int W = 256 / (e->nx / 16);
+    const bool ring = ring_eligible(mode, data, stride, nbatch, bstride, tdata, x);
     if (tm) {
         static const char *mn[] = {"fwd", "inv", "sandwich", "fwd_t", "inv_t"};
-        int st = timer_mark(tm, s, std::string("xcol_kernel<f32,") + std::to_string(e->nx) + "," + mn[mode] + ">",
+        int st = timer_mark(tm, s,
+                            std::string(ring ? "xcol_ring_kernel<f32," : "xcol_kernel<f32,") + std::to_string(e->nx) +
+                                "," + mn[mode] + ">",
                             (double)e->nx * ncols * nbatch * 16.0);
         if (st != FFTB_SUCCESS) return st;
     }
+    if (ring) return launch_xcol_ring(e, mode, data, stride, ncols, nbatch, bstride, tdata, roots, x, s);
     float2 *d = (float2 *)data;
     float2 *td = (float2 *)tdata;
     int nc = (int)ncols;
@@ -829,7 +1032,8 @@ int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz
     if ((st = configure(pe->inv, pe->smem_inv)) != FFTB_SUCCESS) return st;
     for (int m = 0; m < 5; ++m)
         if ((st = configure(xe->fn[m], xe->smem)) != FFTB_SUCCESS ||
-            (st = configure(xe->fn_tc[m], xe->smem_tc)) != FFTB_SUCCESS)
+            (st = configure(xe->fn_tc[m], xe->smem_tc)) != FFTB_SUCCESS ||
+            (m < 3 && (st = configure(xe->fn_ring[m], xe->smem_ring)) != FFTB_SUCCESS))
             return st;
     const int nmax = (int)(ny > nz ? ny : nz);
     if ((st = engine_roots(dtype, nmax, &f.roots_plane)) != FFTB_SUCCESS) return st;
@@ -975,7 +1179,8 @@ int fused4d_init(Fused4D &f, int dtype, int layout, long long nx, long long ny, 
     for (const XColEntry *e : {xe, ye})
         for (int m = 0; m < 5; ++m)
             if ((st = configure(e->fn[m], e->smem)) != FFTB_SUCCESS ||
-                (st = configure(e->fn_tc[m], e->smem_tc)) != FFTB_SUCCESS)
+                (st = configure(e->fn_tc[m], e->smem_tc)) != FFTB_SUCCESS ||
+                (m < 3 && (st = configure(e->fn_ring[m], e->smem_ring)) != FFTB_SUCCESS))
                 return st;
     const int nmax = (int)(nz > nw ? nz : nw);
     if ((st = engine_roots(dtype, nmax, &f.roots_plane)) != FFTB_SUCCESS) return st;

@@ -88,4 +88,45 @@ __device__ __forceinline__ void regfft_warp(cpx<R> (&v)[16], cpx<R> *reg, const 
     }
 }
 
+// Stage twiddles of one thread in registers: tw[k1] = w_N^(t k1), k1 = 1..15 (tw[0] = 1), read
+// from the forward root table `roots` of length nroots (a multiple of N).  A thread whose t
+// is fixed for a whole kernel loads them once instead of reading a table every FFT.
+template <typename R, int N>
+__device__ __forceinline__ void load_stage_twiddles(cpx<R> (&tw)[16], const cpx<R> *roots, int nroots, int t)
+{
+    tw[0] = mk<R>(R(1), R(0));
+#pragma unroll
+    for (int k1 = 1; k1 < 16; ++k1) tw[k1] = roots[((t * k1) % N) * (nroots / N)];
+}
+
+// regfft_warp with the stage twiddles in registers (load_stage_twiddles<R, N> of this t).
+template <typename R, int N, int SIGN>
+__device__ __forceinline__ void regfft_warp_rt(cpx<R> (&v)[16], cpx<R> *reg, const cpx<R> (&tw)[16], int t)
+{
+    using C = cpx<R>;
+    using S = RegFFTShape<N>;
+    constexpr int T = S::T;
+    if constexpr (N <= 16) {
+        dft_small<SIGN, N, C, R>(v);
+    } else {
+        dft16<SIGN, C, R>(v);
+#pragma unroll
+        for (int k1 = 1; k1 < 16; ++k1) v[k1] = SIGN < 0 ? cmul(v[k1], tw[k1]) : cmulc(v[k1], tw[k1]);
+        __syncwarp();
+#pragma unroll
+        for (int k1 = 0; k1 < 16; ++k1) reg[k1 * S::ROWP + t] = v[k1];
+        __syncwarp();
+        constexpr int A = 16 / T;
+#pragma unroll
+        for (int a = 0; a < A; ++a) {
+            C u[T];
+#pragma unroll
+            for (int q = 0; q < T; ++q) u[q] = reg[(t + T * a) * S::ROWP + q];
+            dft_small<SIGN, T, C, R>(u);
+#pragma unroll
+            for (int k2 = 0; k2 < T; ++k2) v[a + A * k2] = u[k2];
+        }
+    }
+}
+
 } // namespace fftb
