@@ -20,11 +20,13 @@
 // through global memory between the z and y stages.
 #include <cooperative_groups.h>
 #include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
+#include <mutex>
 #include <string>
 
 #include "../../include/fftb.h"
@@ -926,17 +928,38 @@ bool ring_eligible(int mode, const void *data, long long stride, long long nbatc
     return true;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point, so the library has no
+// link-time dependency on the driver library (it loads on machines without a GPU)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
 int launch_xcol_ring(const XColEntry *e, int mode, void *data, long long stride, long long ncols, long long nbatch,
                      long long bstride, void *tdata, void *roots, XColEp x, cudaStream_t s)
 {
     const int W = 256 / (e->nx / 16);
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode) {
+        set_last_error("cuTensorMapEncodeTiled is not available from the CUDA driver");
+        return FFTB_ERROR_CUDA;
+    }
     CUtensorMap map;
     const cuuint64_t dims[3] = {(cuuint64_t)(2 * ncols), (cuuint64_t)e->nx, (cuuint64_t)nbatch};
     const cuuint64_t strides[2] = {(cuuint64_t)(stride * 8),
                                    (cuuint64_t)((nbatch > 1 ? bstride : stride * e->nx) * 8)};
     const cuuint32_t box[3] = {(cuuint32_t)(2 * W), (cuuint32_t)e->nx, 1};
     const cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = cuTensorMapEncodeTiled(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, data, dims, strides, box, estr,
+    CUresult r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, data, dims, strides, box, estr,
                                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
