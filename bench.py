@@ -657,6 +657,48 @@ def main():
     except Exception as exc:  # noqa: BLE001
         cufft = {"unavailable": str(exc)[:200]}
 
+    # the reference's own cuFFT ffts path (tests/cufft_ref: the exact cufftMakePlanMany64 plans
+    # of source/ffts.hpp and source/fftm.hpp, auto-allocation off, its transposes and separate
+    # multiply / 1/N kernels) on the same GPU, inputs and flush / event protocol
+    refc = None
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import cufft_ref
+        cufft_ref.build()
+        refc = {"impl": "reference ffts over cuFFT (cufftMakePlanMany64 plans of source/ffts.hpp:677-776, "
+                        "source/fftm.hpp:2941-2961; separate Poisson multiply and 1/N kernels)"}
+        r3 = cufft_ref.RefFfts("float32", (NX, NY, NZ))
+        rspec = torch.empty(ff.spectrum_shape(), dtype=torch.complex64, device=dev)
+        rsol = torch.empty_like(rhs)
+        t = statistics.median(time_events(lambda: r3.poisson(rhs, rspec, rsol, -1.0), 30))
+        refc["poisson_256"] = {"median_us": t * 1e3, "value": BYTES_RT / (t * 1e-3) / 1e9, "unit": "GB/s",
+                               "fftb_speedup": t * 1e3 / statistics.median([x * 1e3 for x in step_ms]),
+                               "rel_l2_vs_fftb": float(torch.linalg.norm(rsol - sol) / torch.linalg.norm(sol))}
+        xr = torch.from_numpy(np.random.default_rng(0).uniform(-1, 1, (NX, NY, NZ)).astype(np.float32)).to(dev)
+        yr = torch.empty_like(xr)
+        t = statistics.median(time_events(lambda: (r3.forward(xr, rspec), r3.backward_normalized(rspec, yr)), 30))
+        refc["roundtrip_256"] = {"median_us": t * 1e3, "value": BYTES_RT / (t * 1e-3) / 1e9, "unit": "GB/s",
+                                 "round_trip_rel_l2": float(torch.linalg.norm(yr - xr) / torch.linalg.norm(xr))}
+        if "median_us" in more.get("roundtrip_256", {}):
+            refc["roundtrip_256"]["fftb_speedup"] = t * 1e3 / more["roundtrip_256"]["median_us"]
+        del r3, rspec, rsol, xr, yr
+        d4 = (64, 64, 64, 64)
+        r4 = cufft_ref.RefFfts("float32", d4, "native_xzwy")
+        x4r = torch.from_numpy(np.random.default_rng(1).standard_normal(d4).astype(np.float32)).to(dev)
+        y4r = torch.empty_like(x4r)
+        s4r = torch.empty((64, 64, 33, 64), dtype=torch.complex64, device=dev)
+        t = statistics.median(time_events(lambda: (r4.forward(x4r, s4r), r4.backward_normalized(s4r, y4r)), 20))
+        b4 = 2 * (4 * 64 ** 4 + 8 * 64 ** 3 * 33)
+        refc["roundtrip4d_64_native"] = {"median_us": t * 1e3, "value": b4 / (t * 1e-3) / 1e9, "unit": "GB/s",
+                                         "round_trip_rel_l2": float(torch.linalg.norm(y4r - x4r) /
+                                                                    torch.linalg.norm(x4r)),
+                                         "note": "the reference waits on the host after each transpose"}
+        if sec and "ms_per_step" in sec:
+            refc["roundtrip4d_64_native"]["fftb_speedup"] = t / sec["ms_per_step"]
+        del r4, x4r, y4r, s4r
+    except Exception as exc:  # noqa: BLE001
+        refc = {"unavailable": str(exc)[:200]}
+
     # accuracy of the timed solution against the analytic solution of the smooth part is not
     # defined (the noise term has no closed form); the CPU leg checks it against the FP64 oracle.
     result = sol.detach().cpu().numpy()
@@ -686,6 +728,7 @@ def main():
                 "serial_value": BYTES_RT * e2e_steps / (e2e_serial_ms * 1e-3) / 1e9,
                 "solutions_identical": e2e_ok},
         "clocks": clk,
+        "reference_cufft": refc,
         "cufft_same_gpu": cufft,
         "secondary": sec,
         "batched": bat,

@@ -1,8 +1,7 @@
-"""Parity with cuFFT on the same GPU and the same seeded inputs: the reference's `ffts`
-forwards every transform to cuFFT (source/external_wrap/cufft_wrap.h), which torch.fft
-wraps as well, so torch.fft.rfftn / irfftn stand in for the reference's cuFFT harness.
-FP32 against FP32: relative L2 <= 2e-6 for spectra and round trips, on the 3D layouts,
-the 4D native_xzwy spectrum [ky][kz][kw][kx], and the Poisson solve."""
+"""Cross-check with torch.fft (cuFFT through torch's own plans) on the same GPU and the same
+seeded inputs, beside the reference-plan harness of test_gpu_cufft_ffts.py: FP32 against
+FP32, relative L2 <= 2e-6 for spectra and round trips, on the 3D layouts, the 4D native_xzwy
+spectrum [ky][kz][kw][kx], and the Poisson solve."""
 import numpy as np
 import pytest
 
