@@ -85,6 +85,11 @@ def version() -> str:
     return _lib.load().fftb_version().decode()
 
 
+def build_digest() -> str:
+    """Digest of the sources the loaded library was compiled from (fftb_build_digest)."""
+    return _lib.load().fftb_build_digest().decode()
+
+
 # ====================================================================== plans
 class Plan:
     """One transform plan (the role of cufft::fft<T, D>).

@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libfftb_b200.so")
 
 # every symbol include/fftb.h declares (checked by the CPU tests)
 EXPORTS = [
-    "fftb_status_string", "fftb_last_error_message", "fftb_version",
+    "fftb_status_string", "fftb_last_error_message", "fftb_version", "fftb_build_digest",
     "fftb_plan_create", "fftb_plan_get_work_size", "fftb_plan_set_work_area", "fftb_plan_set_stream",
     "fftb_exec", "fftb_exec_direction", "fftb_plan_describe", "fftb_plan_num_launches", "fftb_plan_destroy",
     "fftb_ffts_create", "fftb_ffts_destroy", "fftb_ffts_dimension", "fftb_ffts_work_size",
@@ -49,6 +49,7 @@ def load():
     L.fftb_status_string.argtypes = [c_int]
     L.fftb_status_string.restype = ctypes.c_char_p
     L.fftb_version.restype = ctypes.c_char_p
+    L.fftb_build_digest.restype = ctypes.c_char_p
     L.fftb_last_error_message.restype = ctypes.c_char_p
     L.fftb_plan_create.argtypes = [c_int, c_int, c_int, llp, llp, c_ll, c_ll, llp, c_ll, c_ll, c_ll,
                                    ctypes.POINTER(c_vp), szp]
@@ -105,7 +106,7 @@ def load():
     L.fftb_ffts_spectrum_truncate.argtypes = [c_vp, c_vp, c_int, c_int]
     L.fftb_ffts_gradient.argtypes = [c_vp, c_vp, ctypes.POINTER(c_vp)]
     for name in EXPORTS:
-        if name not in ("fftb_status_string", "fftb_version", "fftb_last_error_message"):
+        if name not in ("fftb_status_string", "fftb_version", "fftb_build_digest", "fftb_last_error_message"):
             getattr(L, name).restype = c_int
     _lib = L
     return L

@@ -296,6 +296,11 @@ int fftb_autotune_batch(fftb_batch batch, int op, double sign, const char *cache
 /* Applies FFTB_AUTOTUNE_TILES_SCALE / _CTAS_PER_SM of a config; *mode = FFTB_AUTOTUNE_BATCH_MODE. */
 int fftb_batch_apply_config(fftb_batch batch, const char *text, int *mode);
 
+/* SHA-256 (hex) of the sources the library was compiled from (fftm_b200/csrc and include/),
+ * so a caller can check that the library it loaded matches a source tree.  No counterpart in
+ * the reference (a header-only library, compiled into its caller). */
+const char *fftb_build_digest(void);
+
 /* ------------------------------------------------------------------ allocation-free entry point */
 /* Bytes of the spectrum scratch that fftb_poisson3d_f32_noalloc keeps in static
  * device memory (nx * ny * (nz/2+1) * 8 must not exceed it). */

@@ -47,6 +47,11 @@ def test_version_and_status_strings(lib):
     assert _lib.status_string(-1234) == "unknown status"
 
 
+def test_library_digest_matches_the_sources(lib):
+    from fftm_b200 import build
+    assert lib.fftb_build_digest().decode() == build.source_digest()
+
+
 def test_invalid_plan_arguments_rejected_without_gpu(lib):
     h = ctypes.c_void_p()
     ws = ctypes.c_size_t()
