@@ -636,6 +636,51 @@ def main():
     except Exception as exc:  # noqa: BLE001
         more["derivative_256"] = {"unavailable": str(exc)[:200]}
 
+    # differentiable spectral pipeline at 128^3: u = sin x cos y cos z + 0.05 N(0,1)
+    # (default_rng(4)), w = Poisson(C2R(G R2C(u))) with G = exp(-|k|^2 / (2 16^2)),
+    # loss = 0.5 |w|^2, gradient through the adjoint kernels.  One step = forward + loss +
+    # backward.  Composed: R2C, G multiply (torch), normalised C2R, Poisson solve, and their
+    # adjoints: 4 round trips of algorithmic bytes (2 forward, 2 backward).  Fused: the
+    # filter and Poisson multiply in one sandwich, forward and adjoint: 2 round trips.
+    try:
+        import fftm_b200.autograd as A
+        n3 = (128, 128, 128)
+        g1 = 2 * np.pi * np.arange(128) / 128
+        u0 = (np.sin(g1)[:, None, None] * np.cos(g1)[None, :, None] * np.cos(g1)[None, None, :]
+              + 0.05 * np.random.default_rng(4).standard_normal(n3)).astype(np.float32)
+        f128 = F.ffts("float32").init(*n3)
+        u = torch.from_numpy(u0).to(dev).requires_grad_(True)
+        kx = torch.fft.fftfreq(128, 1.0 / 128, device=dev)
+        kzz = torch.arange(65, device=dev, dtype=torch.float32)
+        G = torch.exp(-(kx[:, None, None] ** 2 + kx[None, :, None] ** 2 + kzz[None, None, :] ** 2)
+                      / (2 * 16.0 ** 2)).to(torch.complex64)
+
+        def composed():
+            u.grad = None
+            w = A.poisson(A.c2r(A.r2c(u, f128) * G, f128, normalized=True), f128, -1.0)
+            (0.5 * (w * w).sum()).backward()
+
+        def fused():
+            u.grad = None
+            w = A.filter_poisson(u, f128, 16.0, -1.0)
+            (0.5 * (w * w).sum()).backward()
+
+        rt128 = 2 * (4 * 128 ** 3 + 8 * 128 * 128 * 65)
+        tc = statistics.median(time_events(composed, 30))
+        gc = u.grad.clone()
+        tf = statistics.median(time_events(fused, 30))
+        gfu = u.grad.clone()
+        more["pipeline_128_grad"] = {
+            "workload": "128^3 f32 loss 0.5|Poisson(C2R(G R2C(u)))|^2, G Gaussian sigma 16, forward + adjoint gradient",
+            "composed": {"median_us": tc * 1e3, "value": 4 * rt128 / (tc * 1e-3) / 1e9, "unit": "GB/s",
+                         "alg_bytes": 4 * rt128},
+            "fused": {"median_us": tf * 1e3, "value": 2 * rt128 / (tf * 1e-3) / 1e9, "unit": "GB/s",
+                      "alg_bytes": 2 * rt128},
+            "grad_rel_l2_fused_vs_composed": float(torch.linalg.norm(gfu - gc) / torch.linalg.norm(gc))}
+        del u, G, gc, gfu, f128
+    except Exception as exc:  # noqa: BLE001
+        more["pipeline_128_grad"] = {"unavailable": str(exc)[:200]}
+
     # batched uneven 3D transforms: 512 shapes with every axis drawn from {32, 48, 64, 96, 128}
     # (numpy default_rng(2)); one step = the R2C + normalised C2R round trip of every transform.
     # The execution mode and knobs come from the autotuner (fresh cache per run): the grouped

@@ -23,7 +23,7 @@ EXPORTS = [
     "fftb_poisson3d_f32_noalloc", "fftb_ffts_forward_adjoint", "fftb_ffts_backward_adjoint",
     "fftb_batch_create", "fftb_batch_destroy", "fftb_batch_layout", "fftb_batch_work_size",
     "fftb_batch_set_work_area", "fftb_batch_set_stream", "fftb_batch_set_tuning", "fftb_batch_exec",
-    "fftb_batch_status", "fftb_batch_describe",
+    "fftb_batch_status", "fftb_batch_describe", "fftb_batch_set_wait_limit", "fftb_batch_wait_selftest",
     "fftb_ffts_set_strategy", "fftb_ffts_get_strategy",
     "fftb_autotune_load_file", "fftb_autotune_save_file", "fftb_autotune_validate", "fftb_autotune_hardware",
     "fftb_autotune_ffts", "fftb_ffts_apply_config", "fftb_autotune_batch", "fftb_batch_apply_config",
@@ -105,6 +105,8 @@ def load():
     L.fftb_ffts_derivative.argtypes = [c_vp, c_vp, c_vp, c_int]
     L.fftb_ffts_spectrum_truncate.argtypes = [c_vp, c_vp, c_int, c_int]
     L.fftb_ffts_gradient.argtypes = [c_vp, c_vp, ctypes.POINTER(c_vp)]
+    L.fftb_batch_set_wait_limit.argtypes = [c_vp, c_ll]
+    L.fftb_batch_wait_selftest.argtypes = [c_ll, ip]
     for name in EXPORTS:
         if name not in ("fftb_status_string", "fftb_version", "fftb_build_digest", "fftb_last_error_message"):
             getattr(L, name).restype = c_int

@@ -121,6 +121,11 @@ class Batch:
         _check(_lib.load().fftb_batch_status(self._h, int(op), ctypes.byref(v)), "fftb_batch_status")
         return v.value
 
+    def set_wait_limit(self, polls: int = 0):
+        """Polls a dependency wait of the persistent launch makes before the error flag
+        (0: the default, about half a second)."""
+        _check(_lib.load().fftb_batch_set_wait_limit(self._h, int(polls)), "fftb_batch_set_wait_limit")
+
     def describe(self, op, sign=-1.0) -> dict:
         vals = [ctypes.c_int() for _ in range(4)]
         _check(_lib.load().fftb_batch_describe(self._h, int(op), float(sign), *[ctypes.byref(v) for v in vals]),
@@ -141,3 +146,11 @@ class Batch:
     def algorithmic_bytes(self) -> int:
         rb = 4 if self.dtype == 0 else 8
         return sum(transform_bytes(s, rb) for s in self.shapes)
+
+
+def wait_selftest(polls: int = 1000) -> int:
+    """Runs the persistent kernel on a work list whose dependency can never be met; its
+    bounded wait must give up after `polls` polls and raise the error flag (returned, 1)."""
+    v = ctypes.c_int()
+    _check(_lib.load().fftb_batch_wait_selftest(int(polls), ctypes.byref(v)), "fftb_batch_wait_selftest")
+    return v.value

@@ -10,8 +10,9 @@
 // every tile of the previous pass of the same transform has been counted done.
 // Because items are taken in list order, every item a CTA waits for has already
 // been taken by a running CTA that waits only on items earlier still, so the wait
-// always ends; it is nevertheless bounded (kSpinLimit polls), after which the
-// kernel raises an error flag that fftb_batch_status reports and every CTA returns.
+// always ends; it is nevertheless bounded (kSpinLimit polls unless the caller set another
+// limit), after which the kernel raises an error flag that fftb_batch_status reports and
+// every CTA returns.
 // The launch (counter reset + kernel) is captured once into a CUDA graph per buffer
 // binding and replayed.
 //
@@ -70,7 +71,8 @@ template <int NF> __device__ __noinline__ void batch_tile(const PassArgs *a, lon
 __global__ void __launch_bounds__(kBatchThreads)
     batch_persistent_kernel(const BatchItem *__restrict__ items, int nitems, const PassArgs *__restrict__ passes,
                             const PassBind *__restrict__ binds, const int *__restrict__ deps,
-                            const int *__restrict__ ntiles, int *ctl, const void *in, void *out, void *work)
+                            const int *__restrict__ ntiles, int *ctl, const void *in, void *out, void *work,
+                            long long spin_limit)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item, s_ok;
@@ -85,7 +87,7 @@ __global__ void __launch_bounds__(kBatchThreads)
                     long long k = 0;
                     while (ld_acquire(&ctl[2 + dp]) < need) {
                         if (ld_acquire(&ctl[1]) != 0) { ok = 0; break; }
-                        if (++k > kSpinLimit) {
+                        if (++k > spin_limit) {
                             atomicExch(&ctl[1], 1);
                             ok = 0;
                             break;
@@ -244,6 +246,7 @@ struct fftb_batch_s {
     cudaStream_t stream = 0;
     int tiles_scale = 1;                      // autotune knob: tiles of G/tiles_scale lines
     int ctas_per_sm = 0;                      // autotune knob: 0 = occupancy limit
+    long long wait_limit = kSpinLimit;        // polls of a dependency wait before the error flag
 };
 
 namespace {
@@ -434,12 +437,13 @@ int build_plan(fftb_batch_s *b, int op, double sign)
     return FFTB_SUCCESS;
 }
 
-int launch_persistent(OpPlan &P, const void *in, void *out, void *work, cudaStream_t s)
+int launch_persistent(OpPlan &P, const void *in, void *out, void *work, cudaStream_t s, long long wait_limit)
 {
     cudaError_t e = cudaMemsetAsync(P.d_ctl, 0, (2 + P.npasses) * sizeof(int), s);
     if (e != cudaSuccess) return set_status_from_cuda(e);
     batch_persistent_kernel<<<P.grid, kBatchThreads, P.smem, s>>>(P.d_items, P.nitems, P.d_passes, P.d_binds,
-                                                                 P.d_deps, P.d_ntiles, P.d_ctl, in, out, work);
+                                                                 P.d_deps, P.d_ntiles, P.d_ctl, in, out, work,
+                                                                 wait_limit);
     return set_status_from_cuda(cudaGetLastError());
 }
 
@@ -570,6 +574,46 @@ int fftb_batch_set_tuning(fftb_batch b, int tiles_scale, int ctas_per_sm)
     return FFTB_SUCCESS;
 }
 
+int fftb_batch_set_wait_limit(fftb_batch b, long long polls)
+{
+    if (!b || polls < 0) return FFTB_ERROR_INVALID_VALUE;
+    b->wait_limit = polls == 0 ? kSpinLimit : polls;
+    for (OpPlan &p : b->ops) free_plan(p);  // captured graphs hold the old limit
+    return FFTB_SUCCESS;
+}
+
+// The persistent kernel on a one-item work list whose producer pass has no items: its
+// dependency wait can only end by running out of polls, which must raise the error flag and
+// return.  Checks the bounded-wait path without faulting or hanging anything.
+int fftb_batch_wait_selftest(long long polls, int *error_flag)
+{
+    if (!error_flag || polls < 1) return FFTB_ERROR_INVALID_VALUE;
+    *error_flag = 0;
+    const BatchItem item = {1, 0};
+    const int deps[2] = {-1, 0}, ntiles[2] = {1, 1};
+    const size_t off_args = 256, off_binds = off_args + 2 * sizeof(PassArgs), off_deps = off_binds + 2 * sizeof(PassBind);
+    const size_t off_nt = off_deps + 64, off_ctl = off_nt + 64, total = off_ctl + 64;
+    char *blob = nullptr;
+    cudaError_t e = cudaMalloc(&blob, total);
+    if (e != cudaSuccess) return set_status_from_cuda(e);
+    if (e == cudaSuccess) e = cudaMemset(blob, 0, total);
+    if (e == cudaSuccess) e = cudaMemcpy(blob, &item, sizeof(item), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(blob + off_deps, deps, sizeof(deps), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(blob + off_nt, ntiles, sizeof(ntiles), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        int *ctl = (int *)(blob + off_ctl);
+        batch_persistent_kernel<<<1, kBatchThreads, 0>>>((const BatchItem *)blob, 1, (const PassArgs *)(blob + off_args),
+                                                         (const PassBind *)(blob + off_binds),
+                                                         (const int *)(blob + off_deps), (const int *)(blob + off_nt),
+                                                         ctl, nullptr, nullptr, nullptr, polls);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaMemcpy(error_flag, ctl + 1, sizeof(int), cudaMemcpyDeviceToHost);
+    }
+    cudaFree(blob);
+    return set_status_from_cuda(e);
+}
+
 int fftb_batch_exec(fftb_batch b, int op, const void *in, void *out, double sign, int mode)
 {
     if (!b) return FFTB_ERROR_INVALID_HANDLE;
@@ -587,7 +631,7 @@ int fftb_batch_exec(fftb_batch b, int op, const void *in, void *out, double sign
         return program_exec(P.seq, const_cast<void *>(in), out, work, b->stream);
     }
     if ((uintptr_t)in % 16 || (uintptr_t)out % 16 || (uintptr_t)work % 16) return FFTB_ERROR_MISALIGNED;
-    if (mode == 1) return launch_persistent(P, in, out, work, b->stream);
+    if (mode == 1) return launch_persistent(P, in, out, work, b->stream, b->wait_limit);
     if (mode == 3) return launch_groups(P, in, out, work, b->stream);
     // modes 2 and 4: replay the captured graph (captured on first use of this binding)
     if (!P.gexec || P.g_mode != mode || P.g_in != in || P.g_out != out || P.g_work != work) {
@@ -600,7 +644,7 @@ int fftb_batch_exec(fftb_batch b, int op, const void *in, void *out, double sign
         if (e != cudaSuccess) return set_status_from_cuda(e);
         e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            st = mode == 2 ? launch_persistent(P, in, out, work, cap) : launch_groups(P, in, out, work, cap);
+            st = mode == 2 ? launch_persistent(P, in, out, work, cap, b->wait_limit) : launch_groups(P, in, out, work, cap);
             cudaGraph_t g = nullptr;
             e = cudaStreamEndCapture(cap, &g);
             if (st == FFTB_SUCCESS && e == cudaSuccess) {

@@ -243,6 +243,14 @@ int fftb_batch_exec(fftb_batch batch, int op, const void *in, void *out, double 
 /* error flag of the last persistent launch of op: 1 if a dependency wait ran out its
  * bounded number of polls (the launch then returned early); synchronises the device. */
 int fftb_batch_status(fftb_batch batch, int op, int *error_flag);
+/* Polls a dependency wait of the persistent launch makes before it raises the error flag and
+ * every CTA returns (0 restores the default, 2^22 polls, about half a second).  Cached CUDA
+ * graphs of the batch are rebuilt. */
+int fftb_batch_set_wait_limit(fftb_batch batch, long long polls);
+/* Self-test of that bounded wait: the persistent kernel on a one-item work list whose
+ * producer has no items waits `polls` polls, raises the flag and returns; *error_flag
+ * receives it (1 when the path works).  Faults and hangs nothing; the context stays usable. */
+int fftb_batch_wait_selftest(long long polls, int *error_flag);
 int fftb_batch_describe(fftb_batch batch, int op, double sign, int *passes, int *items, int *grid,
                         int *persistent);
 

@@ -98,6 +98,50 @@ def test_batch_full_workload_512(B, torch_cuda):
 
 
 
+def test_batch_full_workload_512_forward_spectra_vs_oracle(B, torch_cuda):
+    # the benchmarked form (grouped launches replayed from a graph, mode 4) on the full
+    # 512-shape workload: forward spectra of a sample of transforms of every length mix
+    # against the FP64 oracle, and the round trip of all of them
+    torch = torch_cuda
+    shapes = B.draw_shapes(512, seed=2)
+    b = B.Batch(shapes)
+    x, host = _fill(torch, b, 9)
+    spec = torch.zeros(b.spectrum_total, dtype=torch.complex64, device="cuda")
+    b.exec(B.FORWARD, x, spec, mode=B.GROUPED_GRAPH)
+    torch.cuda.synchronize()
+    sp = spec.cpu().numpy()
+    for i in list(range(0, 512, 37)) + [511]:
+        s = shapes[i]
+        o, so = b.real_offsets[i], b.spectrum_offsets[i]
+        xi = host[o:o + int(np.prod(s))].reshape(s).astype(np.float64)
+        got = sp[so:so + s[0] * s[1] * (s[2] // 2 + 1)].reshape(s[0], s[1], s[2] // 2 + 1)
+        assert O.rel_l2(got.astype(np.complex128), O.ffts3d_forward(xi)) <= TOL, (i, s)
+    out = torch.zeros_like(x)
+    b.exec(B.ROUNDTRIP, x, out, mode=B.GROUPED_GRAPH)
+    torch.cuda.synchronize()
+    assert float(torch.linalg.norm(out - x) / torch.linalg.norm(x)) <= TOL
+
+
+def test_bounded_dependency_wait_gives_up_and_flags(B, torch_cuda):
+    # a wait on a producer that has no items (nothing ever counts it done) must run out of
+    # polls, raise the error flag and return; the context stays usable afterwards
+    torch = torch_cuda
+    import time
+    t0 = time.time()
+    assert B.wait_selftest(2000) == 1
+    assert time.time() - t0 < 30
+    shapes = B.draw_shapes(6, seed=2)
+    b = B.Batch(shapes)
+    b.set_wait_limit(1 << 20)
+    x, host = _fill(torch, b, 3)
+    out = torch.zeros_like(x)
+    b.exec(B.ROUNDTRIP, x, out, mode=B.PERSISTENT)
+    torch.cuda.synchronize()
+    assert b.status(B.ROUNDTRIP) == 0
+    assert float(torch.linalg.norm(out - x) / torch.linalg.norm(x)) <= TOL
+    b.set_wait_limit(0)
+
+
 def test_batch_float64_runs_sequential_launches(B, torch_cuda):
     torch = torch_cuda
     shapes = [(16, 12, 10), (9, 8, 14), (32, 16, 8)]
