@@ -239,6 +239,59 @@ class fft_wrap_many:
 
 
 # ====================================================================== ffts
+class ffts_init_options:
+    """The reference's ffts_init_options (source/ffts.hpp:64-72), with its defaults: both
+    profilers on (keys "ffts_prof" / "ffts_mem") and every report printed on destroy.  An
+    empty key turns that profiler off."""
+
+    def __init__(self, profiling_key="ffts_prof", memory_profiling_key="ffts_mem",
+                 print_profile_summary_on_destroy=True, print_profile_totals_on_destroy=True,
+                 print_memory_profile_on_destroy=True, print_memory_totals_on_destroy=True):
+        self.profiling_key = profiling_key
+        self.memory_profiling_key = memory_profiling_key
+        self.print_profile_summary_on_destroy = print_profile_summary_on_destroy
+        self.print_profile_totals_on_destroy = print_profile_totals_on_destroy
+        self.print_memory_profile_on_destroy = print_memory_profile_on_destroy
+        self.print_memory_totals_on_destroy = print_memory_totals_on_destroy
+
+    def _c(self):
+        o = _lib.InitOptions()
+        o.profiling_key = (self.profiling_key or "").encode()
+        o.memory_profiling_key = (self.memory_profiling_key or "").encode()
+        o.print_profile_summary_on_destroy = int(bool(self.print_profile_summary_on_destroy))
+        o.print_profile_totals_on_destroy = int(bool(self.print_profile_totals_on_destroy))
+        o.print_memory_profile_on_destroy = int(bool(self.print_memory_profile_on_destroy))
+        o.print_memory_totals_on_destroy = int(bool(self.print_memory_totals_on_destroy))
+        return o
+
+
+class fftm_reporting_options:
+    """fftm's reporting options (source/fftm_options.hpp:220-241), defaults all off; the
+    single-GPU path maps them onto ffts_init_options (to_ffts_init_options)."""
+
+    def __init__(self, profiling_key="", memory_profiling_key="", verbose=False,
+                 print_profile_summary_on_destroy=False, print_profile_totals_on_destroy=False,
+                 print_memory_profile_on_destroy=False, print_memory_totals_on_destroy=False):
+        self.profiling_key = profiling_key
+        self.memory_profiling_key = memory_profiling_key
+        self.verbose = verbose
+        self.print_profile_summary_on_destroy = print_profile_summary_on_destroy
+        self.print_profile_totals_on_destroy = print_profile_totals_on_destroy
+        self.print_memory_profile_on_destroy = print_memory_profile_on_destroy
+        self.print_memory_totals_on_destroy = print_memory_totals_on_destroy
+
+    def to_ffts_init_options(self) -> ffts_init_options:
+        return ffts_init_options(self.profiling_key, self.memory_profiling_key,
+                                 self.print_profile_summary_on_destroy, self.print_profile_totals_on_destroy,
+                                 self.print_memory_profile_on_destroy, self.print_memory_totals_on_destroy)
+
+
+def profiling_reporting_options() -> fftm_reporting_options:
+    """fftm's profiling preset (source/fftm_options.hpp:231-242): keys "fftm_prof" /
+    "fftm_mem", every report printed on destroy."""
+    return fftm_reporting_options("fftm_prof", "fftm_mem", False, True, True, True, True)
+
+
 class ffts:
     """The single-GPU frontend (fftm::ffts, source/ffts.hpp:159-383).
 
@@ -253,13 +306,21 @@ class ffts:
         self._dims = None
         self._work = None
 
-    def init(self, nx, ny, nz=None, nw=None):
+    def init(self, nx, ny, nz=None, nw=None, options=None):
+        """``options``: an ``ffts_init_options`` (profiling keys and print-on-destroy flags);
+        None keeps both profilers off (the C++ layer defaults to the reference's options,
+        which print on destroy)."""
         if self._h is not None:
             raise LogicError("ffts::init can only be called once per instance.")
         L = _lib.load()
         h = ctypes.c_void_p()
-        _check(L.fftb_ffts_create(self.dtype, nx, ny, nz or 0, nw or 0, self.strategy_4d, ctypes.byref(h)),
-               "ffts::init")
+        if options is None:
+            _check(L.fftb_ffts_create(self.dtype, nx, ny, nz or 0, nw or 0, self.strategy_4d, ctypes.byref(h)),
+                   "ffts::init")
+        else:
+            o = options._c()
+            _check(L.fftb_ffts_create_ex(self.dtype, nx, ny, nz or 0, nw or 0, self.strategy_4d, ctypes.byref(o),
+                                         ctypes.byref(h)), "ffts::init")
         self._h = h
         self._dims = tuple(d for d in (nx, ny, nz, nw) if d)
         ws = ctypes.c_size_t()
@@ -278,6 +339,18 @@ class ffts:
 
     def is_initialized(self) -> bool:
         return self._h is not None
+
+    def profile_report(self, which="summary") -> str:
+        """The profilers' reports as text: "summary", "totals", "memory" or "memory_totals"
+        (empty when that profiler is off)."""
+        self._ensure()
+        w = {"summary": 0, "totals": 1, "memory": 2, "memory_totals": 3}[which]
+        L = _lib.load()
+        need = ctypes.c_size_t()
+        _check(L.fftb_ffts_profile_report(self._h, w, None, 0, ctypes.byref(need)), "profile_report")
+        buf = ctypes.create_string_buffer(need.value)
+        _check(L.fftb_ffts_profile_report(self._h, w, buf, need.value, ctypes.byref(need)), "profile_report")
+        return buf.value.decode()
 
     def _ensure(self, dim=None):
         if self._h is None:

@@ -16,7 +16,8 @@ EXPORTS = [
     "fftb_status_string", "fftb_last_error_message", "fftb_version", "fftb_build_digest",
     "fftb_plan_create", "fftb_plan_get_work_size", "fftb_plan_set_work_area", "fftb_plan_set_stream",
     "fftb_exec", "fftb_exec_direction", "fftb_plan_describe", "fftb_plan_num_launches", "fftb_plan_destroy",
-    "fftb_ffts_create", "fftb_ffts_destroy", "fftb_ffts_dimension", "fftb_ffts_work_size",
+    "fftb_ffts_create", "fftb_ffts_create_ex", "fftb_ffts_profile_report", "fftb_init_options_default",
+    "fftb_ffts_destroy", "fftb_ffts_dimension", "fftb_ffts_work_size",
     "fftb_ffts_set_work_area", "fftb_ffts_set_stream", "fftb_ffts_forward", "fftb_ffts_backward",
     "fftb_ffts_backward_normalized", "fftb_ffts_poisson", "fftb_ffts_filter", "fftb_ffts_spectrum_poisson",
     "fftb_ffts_num_launches", "fftb_ffts_timing_enable", "fftb_ffts_timing_read",
@@ -25,12 +26,19 @@ EXPORTS = [
     "fftb_batch_set_work_area", "fftb_batch_set_stream", "fftb_batch_set_tuning", "fftb_batch_exec",
     "fftb_batch_status", "fftb_batch_describe", "fftb_batch_set_wait_limit", "fftb_batch_wait_selftest",
     "fftb_ffts_set_strategy", "fftb_ffts_get_strategy",
-    "fftb_autotune_load_file", "fftb_autotune_save_file", "fftb_autotune_validate", "fftb_autotune_hardware",
+    "fftb_autotune_load_file", "fftb_autotune_save_file", "fftb_autotune_validate", "fftb_autotune_hardware", "fftb_autotune_signature",
     "fftb_autotune_ffts", "fftb_ffts_apply_config", "fftb_autotune_batch", "fftb_batch_apply_config",
     "fftb_ffts_spectrum_derivative", "fftb_ffts_derivative", "fftb_ffts_spectrum_truncate", "fftb_ffts_gradient",
 ]
 
 _lib = None
+
+
+class InitOptions(ctypes.Structure):
+    """fftb_init_options (include/fftb.h): the reference's ffts_init_options."""
+    _fields_ = [("profiling_key", ctypes.c_char_p), ("memory_profiling_key", ctypes.c_char_p),
+                ("print_profile_summary_on_destroy", ctypes.c_int), ("print_profile_totals_on_destroy", ctypes.c_int),
+                ("print_memory_profile_on_destroy", ctypes.c_int), ("print_memory_totals_on_destroy", ctypes.c_int)]
 
 
 def load():
@@ -97,6 +105,7 @@ def load():
     L.fftb_autotune_save_file.argtypes = [cp, cp]
     L.fftb_autotune_validate.argtypes = [cp, cp, c_int]
     L.fftb_autotune_hardware.argtypes = [c_int, cp, c_sz, szp]
+    L.fftb_autotune_signature.argtypes = [cp, cp, c_sz, szp]
     L.fftb_autotune_ffts.argtypes = [c_int, c_ll, c_ll, c_ll, c_ll, c_int, cp, c_int, c_int, c_int, cp, c_sz, szp, ip]
     L.fftb_ffts_apply_config.argtypes = [c_vp, cp]
     L.fftb_autotune_batch.argtypes = [c_vp, c_int, c_d, cp, c_int, c_int, c_int, cp, c_sz, szp, ip, ip]
@@ -107,9 +116,14 @@ def load():
     L.fftb_ffts_gradient.argtypes = [c_vp, c_vp, ctypes.POINTER(c_vp)]
     L.fftb_batch_set_wait_limit.argtypes = [c_vp, c_ll]
     L.fftb_batch_wait_selftest.argtypes = [c_ll, ip]
+    L.fftb_ffts_create_ex.argtypes = [c_int, c_ll, c_ll, c_ll, c_ll, c_int, ctypes.POINTER(InitOptions),
+                                      ctypes.POINTER(c_vp)]
+    L.fftb_ffts_profile_report.argtypes = [c_vp, c_int, cp, c_sz, szp]
+    L.fftb_init_options_default.argtypes = [ctypes.POINTER(InitOptions)]
     for name in EXPORTS:
         if name not in ("fftb_status_string", "fftb_version", "fftb_build_digest", "fftb_last_error_message"):
             getattr(L, name).restype = c_int
+    L.fftb_init_options_default.restype = None
     _lib = L
     return L
 

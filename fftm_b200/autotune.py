@@ -126,6 +126,13 @@ def hardware_config(device: int = 0) -> dict:
     return parse_text(buf.value.decode())
 
 
+def signature(canonical: str) -> str:
+    """"v2:" + 64-bit FNV-1a of a canonical hardware description (the reference's hash)."""
+    buf, _, st = _text_call(_lib.load().fftb_autotune_signature, canonical.encode())
+    _check(st, "signature")
+    return buf.value.decode()
+
+
 def load_or_measure_config(dtype, sizes, options: autotune_options, measured: measured_options | None = None,
                            strategy_4d="pencil") -> selected_config:
     """Uses the cache when it matches the problem and this GPU; otherwise measures the

@@ -21,6 +21,8 @@
 // per SM.
 #include <cuda_runtime.h>
 
+#include <cctype>
+
 #include <sys/stat.h>
 
 #include <algorithm>
@@ -170,38 +172,86 @@ std::string fnv1a_hex(const std::string &s)
 }
 
 // --------------------------------------------------------------------------- hardware
+// The hardware signature is the reference's, for one rank, so that a cache fftm wrote on
+// this machine validates here and the other way round
+// (source/detail/fftm_autotune_hardware.inc:28-97 token rules, :101-124 device class and
+// transport environment, :285-310 canonical strings, :312-343 metadata keys): the
+// compatibility string names the rank count, node layout, MPI library ("unavailable"
+// without MPI), device class (backend, model, compute capability, memory, runtime and
+// driver versions), transport ("local") and transport environment; the strict string adds
+// device UUIDs, PCI bus ids and node names ("local").  Each is hashed with 64-bit FNV-1a.
+
+// separators (NUL, white space, ';', '=', ',', '|') become one '_', none at the ends
+std::string hw_token(const std::string &v)
+{
+    std::string r;
+    bool prev = false;
+    for (unsigned char ch : v) {
+        const bool sep = ch == '\0' || std::isspace(ch) || ch == ';' || ch == '=' || ch == ',' || ch == '|';
+        if (sep) {
+            if (!r.empty() && !prev) r.push_back('_');
+            prev = true;
+            continue;
+        }
+        r.push_back((char)ch);
+        prev = false;
+    }
+    while (!r.empty() && r.back() == '_') r.pop_back();
+    return r.empty() ? "unknown" : r;
+}
+
+std::string hw_env(const char *name)
+{
+    const char *v = getenv(name);
+    return hw_token(v ? v : "default");
+}
+
 int hardware_config(int device, Config &c)
 {
     cudaDeviceProp p;
     cudaError_t e = cudaGetDeviceProperties(&p, device);
     if (e != cudaSuccess) return set_status_from_cuda(e);
-    int rt = 0, drv = 0, ndev = 0;
+    int rt = 0, drv = 0;
     cudaRuntimeGetVersion(&rt);
     cudaDriverGetVersion(&drv);
-    cudaGetDeviceCount(&ndev);
     char uuid[40];
     for (int i = 0; i < 16; ++i) snprintf(uuid + 2 * i, 3, "%02x", (unsigned char)p.uuid.bytes[i]);
-    char pci[32];
-    snprintf(pci, sizeof(pci), "%04x:%02x:%02x.0", p.pciDomainID, p.pciBusID, p.pciDeviceID);
-    const std::string arch = "sm_" + std::to_string(p.major) + std::to_string(p.minor);
-    // a device class: what makes a tuned choice transferable between two GPUs
-    const std::string cls = std::string(p.name) + "/" + arch + "/sms=" + std::to_string(p.multiProcessorCount) +
-                            "/smem=" + std::to_string(p.sharedMemPerBlockOptin) +
-                            "/l2=" + std::to_string(p.l2CacheSize) + "/mem=" + std::to_string(p.totalGlobalMem);
-    const std::string compat = "version=2;gpus=1;device_classes=" + cls + ";runtime=" + std::to_string(rt);
-    const std::string strict = compat + ";device_uuids=" + uuid + ";pci_bus_ids=" + pci;
+    char pci[32] = {};
+    if (cudaDeviceGetPCIBusId(pci, (int)sizeof(pci), device) != cudaSuccess) {
+        cudaGetLastError();
+        snprintf(pci, sizeof(pci), "unavailable");
+    }
+    const std::string arch = std::to_string(p.major) + "." + std::to_string(p.minor);
+    const std::string cls = "backend=cuda:model=" + hw_token(p.name) + ":arch=" + hw_token(arch) +
+                            ":memory=" + std::to_string((unsigned long long)p.totalGlobalMem) +
+                            ":runtime=" + std::to_string(rt) + ":driver=" + std::to_string(drv);
+    const std::string env = "affinity=" + hw_env("FFTM_MPI_RANK_AFFINITY_MODE") + ":ucx_tls=" + hw_env("UCX_TLS") +
+                            ":ucx_net_devices=" + hw_env("UCX_NET_DEVICES") + ":mpi_pml=" + hw_env("OMPI_MCA_pml") +
+                            ":mpi_btl=" + hw_env("OMPI_MCA_btl");
+    const std::string compat = "version=2;mpi_ranks=1;node_count=1;ranks_per_node=1;devices_per_node=1"
+                               ";mpi_library=unavailable;device_classes=" + hw_token(cls) +
+                               ";transport=local;transport_env=" + hw_token(env);
+    const std::string strict = compat + ";device_uuids=" + hw_token(uuid) + ";pci_bus_ids=" + hw_token(pci) +
+                               ";nodes=local";
     c["FFTM_AUTOTUNE_HARDWARE_SIGNATURE_VERSION"] = "2";
     c["FFTM_AUTOTUNE_HARDWARE_SIGNATURE"] = "v2:" + fnv1a_hex(compat);
     c["FFTM_AUTOTUNE_HARDWARE_SIGNATURE_STRICT"] = "v2:" + fnv1a_hex(strict);
     c["FFTM_AUTOTUNE_HARDWARE_BACKENDS"] = "cuda";
-    c["FFTM_AUTOTUNE_GPU_MODELS"] = p.name;
-    c["FFTM_AUTOTUNE_GPU_ARCHITECTURES"] = arch;
-    c["FFTM_AUTOTUNE_DEVICE_UUIDS"] = uuid;
-    c["FFTM_AUTOTUNE_DEVICE_PCI_BUS_IDS"] = pci;
-    c["FFTM_AUTOTUNE_DEVICE_TOTAL_BYTES"] = std::to_string(p.totalGlobalMem);
+    c["FFTM_AUTOTUNE_GPU_MODELS"] = hw_token(p.name);
+    c["FFTM_AUTOTUNE_GPU_ARCHITECTURES"] = hw_token(arch);
+    c["FFTM_AUTOTUNE_DEVICE_UUIDS"] = hw_token(uuid);
+    c["FFTM_AUTOTUNE_DEVICE_PCI_BUS_IDS"] = hw_token(pci);
+    c["FFTM_AUTOTUNE_DEVICE_TOTAL_BYTES"] = std::to_string((unsigned long long)p.totalGlobalMem);
     c["FFTM_AUTOTUNE_RUNTIME_VERSIONS"] = std::to_string(rt);
     c["FFTM_AUTOTUNE_DRIVER_VERSIONS"] = std::to_string(drv);
-    c["FFTM_AUTOTUNE_DEVICES_PER_NODE"] = std::to_string(ndev);
+    c["FFTM_AUTOTUNE_MPI_LIBRARY"] = "unavailable";
+    c["FFTM_AUTOTUNE_NODE_COUNT"] = "1";
+    c["FFTM_AUTOTUNE_RANKS_PER_NODE"] = "1";
+    c["FFTM_AUTOTUNE_DEVICES_PER_NODE"] = "1";
+    c["FFTM_AUTOTUNE_NODE_NAMES"] = "local";
+    c["FFTM_AUTOTUNE_TRANSPORT"] = "local";
+    c["FFTM_AUTOTUNE_TRANSPORT_ENVIRONMENT"] = hw_token(env);
+    c["FFTB_AUTOTUNE_CANONICAL_COMPATIBILITY"] = compat;
     return FFTB_SUCCESS;
 }
 
@@ -215,8 +265,50 @@ const char *kIdentityKeys[] = {
     "FFTB_AUTOTUNE_BATCH_SHAPES", "FFTB_AUTOTUNE_BATCH_OP",
 };
 
+int validate_hardware(const Config &cache, const Config &expect, int flags);
+
+// A cache the reference wrote for one GPU (FFTM_AUTOTUNE_LIBRARY=fftm: its policy or measured
+// cache, source/fftm_autotune.hpp:660-676): schema 2, the same dimension, sizes and one rank,
+// and the same hardware.  Its strategy keys name MPI decompositions (slab-pencil,
+// pencil-slab, pencil-pencil in 3D; slab-slab, pencil-pencil in 4D) that all reduce to the
+// one single-GPU transform, so they map onto this library's own default execution.
+int validate_reference(const Config &cache, const Config &expect, int flags)
+{
+    const char *keys[] = {"FFTM_AUTOTUNE_SCHEMA", "FFTM_AUTOTUNE_DIM", "FFTM_AUTOTUNE_NUM_GPUS",
+                          "FFTM_AUTOTUNE_SIZE_2D", "FFTM_AUTOTUNE_SIZE_3D", "FFTM_AUTOTUNE_SIZE_4D"};
+    for (const char *k : keys) {
+        auto it = expect.find(k);
+        if (it == expect.end()) continue;
+        if (get(cache, k) != it->second) {
+            set_last_error(std::string("fftm autotune cache ") + k + "='" + get(cache, k) + "' does not match '" +
+                           it->second + "'");
+            return FFTB_ERROR_CACHE_MISMATCH;
+        }
+    }
+    if (expect.count("FFTB_AUTOTUNE_BATCH_COUNT")) {
+        set_last_error("an fftm autotune cache has no batched form");
+        return FFTB_ERROR_CACHE_MISMATCH;
+    }
+    return validate_hardware(cache, expect, flags);
+}
+
+// The fftb config that a validated reference cache stands for: the problem and hardware
+// keys of `expect`, the default execution, and the reference's choice kept for the record.
+Config translate_reference(const Config &cache, const Config &expect)
+{
+    Config c = expect;
+    c["FFTM_AUTOTUNE_SOURCE"] = "fftm-cache:" + get(cache, "FFTM_AUTOTUNE_SOURCE");
+    c["FFTB_AUTOTUNE_STRATEGY"] = "auto";
+    c["FFTB_AUTOTUNE_PLANE_CLUSTER"] = "0";
+    const std::string s3 = get(cache, "FFTM_AUTOTUNE_STRATEGY_3D"), s4 = get(cache, "FFTM_AUTOTUNE_STRATEGY_4D");
+    if (!s3.empty()) c["FFTB_AUTOTUNE_REFERENCE_STRATEGY_3D"] = s3;
+    if (!s4.empty()) c["FFTB_AUTOTUNE_REFERENCE_STRATEGY_4D"] = s4;
+    return c;
+}
+
 int validate(const Config &cache, const Config &expect, int flags)
 {
+    if (get(cache, "FFTM_AUTOTUNE_LIBRARY") == "fftm") return validate_reference(cache, expect, flags);
     for (const char *k : kIdentityKeys) {
         auto it = expect.find(k);
         if (it == expect.end()) continue;
@@ -231,6 +323,11 @@ int validate(const Config &cache, const Config &expect, int flags)
                        get(cache, "FFTM_AUTOTUNE_SOURCE") + "')");
         return FFTB_ERROR_CACHE_MISMATCH;
     }
+    return validate_hardware(cache, expect, flags);
+}
+
+int validate_hardware(const Config &cache, const Config &expect, int flags)
+{
     if (!(flags & FFTB_TUNE_NO_HARDWARE_CHECK)) {
         const std::string sig = get(cache, "FFTM_AUTOTUNE_HARDWARE_SIGNATURE");
         if (sig.rfind("v2:", 0) != 0) {
@@ -719,7 +816,7 @@ int load_or_measure(const char *cache_file, int flags, int device, const Config 
             st = load_file(path, cached);
             if (st == FFTB_SUCCESS) st = validate(cached, expect, flags);
             if (st == FFTB_SUCCESS) {
-                result = cached;
+                result = get(cached, "FFTM_AUTOTUNE_LIBRARY") == "fftm" ? translate_reference(cached, expect) : cached;
                 if (from_cache) *from_cache = 1;
                 return FFTB_SUCCESS;
             }
@@ -768,6 +865,12 @@ int fftb_autotune_validate(const char *cache_text, const char *expected_text, in
     return st;
 }
 
+int fftb_autotune_signature(const char *canonical, char *text, size_t capacity, size_t *needed)
+{
+    if (!canonical) return FFTB_ERROR_INVALID_VALUE;
+    return put_text("v2:" + fnv1a_hex(canonical), text, capacity, needed);
+}
+
 int fftb_autotune_hardware(int device, char *text, size_t capacity, size_t *needed)
 {
     Config c;
@@ -804,13 +907,15 @@ int fftb_ffts_apply_config(fftb_ffts obj, const char *text)
     if (st != FFTB_SUCCESS) return st;
     const std::string strat = get(c, "FFTB_AUTOTUNE_STRATEGY");
     int cl = 0;
-    if ((strat != "fused" && strat != "fused_tc" && strat != "staged") ||
+    if ((strat != "fused" && strat != "fused_tc" && strat != "staged" && strat != "auto") ||
         to_int(get(c, "FFTB_AUTOTUNE_PLANE_CLUSTER"), &cl) != FFTB_SUCCESS) {
         set_last_error("autotune config has no valid FFTB_AUTOTUNE_STRATEGY / FFTB_AUTOTUNE_PLANE_CLUSTER");
         return FFTB_ERROR_CACHE_MISMATCH;
     }
-    const int code =
-        strat == "fused" ? FFTB_STRATEGY_FUSED : (strat == "fused_tc" ? FFTB_STRATEGY_FUSED_TC : FFTB_STRATEGY_STAGED);
+    const int code = strat == "fused"      ? FFTB_STRATEGY_FUSED
+                     : strat == "fused_tc" ? FFTB_STRATEGY_FUSED_TC
+                     : strat == "auto"     ? FFTB_STRATEGY_AUTO
+                                           : FFTB_STRATEGY_STAGED;
     return fftb_ffts_set_strategy(obj, code, cl);
 }
 

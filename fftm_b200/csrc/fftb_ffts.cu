@@ -8,13 +8,16 @@
 // the epilogue of the final C2R pass.
 #include <cuda_runtime.h>
 
+#include <cstdio>
 #include <cstring>
 #include <new>
+#include <string>
 
 #include "../../include/fftb.h"
 #include "fftb_device.cuh"
 #include "fftb_engine.h"
 #include "fftb_fused3d.h"
+#include "fftb_profile.h"
 
 using namespace fftb;
 
@@ -33,6 +36,11 @@ struct fftb_ffts_s {
     bool timing = false;
     void *dspec = nullptr;  // spectrum buffers of the derivative calls (allocated on first use)
     void *dspec2 = nullptr;
+    size_t dspec_bytes = 0;
+    // profiling (ffts_init_options): scopes per API call, memory entries, print flags
+    Profiler prof;
+    MemProfiler mem;
+    int print_flags = 0;  // bit 0 profile summary, 1 profile totals, 2 memory profile, 3 memory totals
 };
 
 namespace {
@@ -319,6 +327,7 @@ int ensure_work(fftb_ffts_s *o)
     }
     o->work = p;
     o->own_work = true;
+    o->mem.set_bytes("ffts/shared_work_buffer", (long long)o->work_bytes);
     return FFTB_SUCCESS;
 }
 
@@ -453,9 +462,37 @@ void spectrum_geometry(const fftb_ffts_s *o, int4 &dims, int4 &ns, int &half_axi
 
 } // namespace
 
+namespace {
+// "ffts::<what><D>" scope names of the profiler (built only when profiling is on)
+std::string scope_name(const fftb_ffts_s *o, const char *what)
+{
+    return std::string("ffts::") + what + "<" + std::to_string(o->dim) + ">";
+}
+} // namespace
+#define FFTB_PROFILE_SCOPE(o, what)                                                                                   \
+    ProfScope _prof_scope((o)->prof, (o)->prof.enabled ? scope_name((o), (what)) : std::string(), (o)->stream)
+
 extern "C" {
 
+void fftb_init_options_default(fftb_init_options *opt)
+{
+    if (!opt) return;
+    opt->profiling_key = "ffts_prof";
+    opt->memory_profiling_key = "ffts_mem";
+    opt->print_profile_summary_on_destroy = 1;
+    opt->print_profile_totals_on_destroy = 1;
+    opt->print_memory_profile_on_destroy = 1;
+    opt->print_memory_totals_on_destroy = 1;
+}
+
 int fftb_ffts_create(int dtype, long long nx, long long ny, long long nz, long long nw, int layout4d, fftb_ffts *obj)
+{
+    fftb_init_options off = {nullptr, nullptr, 0, 0, 0, 0};
+    return fftb_ffts_create_ex(dtype, nx, ny, nz, nw, layout4d, &off, obj);
+}
+
+int fftb_ffts_create_ex(int dtype, long long nx, long long ny, long long nz, long long nw, int layout4d,
+                        const fftb_init_options *options, fftb_ffts *obj)
 {
     if (!obj) return FFTB_ERROR_INVALID_VALUE;
     *obj = nullptr;
@@ -470,13 +507,31 @@ int fftb_ffts_create(int dtype, long long nx, long long ny, long long nz, long l
     o->nw = nw;
     o->layout = layout4d;
     o->dim = nz == 0 ? 2 : (nw == 0 ? 3 : 4);
+    fftb_init_options defaults;
+    fftb_init_options_default(&defaults);
+    const fftb_init_options &op = options ? *options : defaults;
+    if (op.profiling_key && op.profiling_key[0]) {
+        o->prof.enabled = true;
+        o->prof.key = op.profiling_key;
+    }
+    if (op.memory_profiling_key && op.memory_profiling_key[0]) {
+        o->mem.enabled = true;
+        o->mem.key = op.memory_profiling_key;
+        o->mem.set_bytes("ffts/shared_work_buffer", 0);
+    }
+    o->print_flags = (op.print_profile_summary_on_destroy ? 1 : 0) | (op.print_profile_totals_on_destroy ? 2 : 0) |
+                     (op.print_memory_profile_on_destroy ? 4 : 0) | (op.print_memory_totals_on_destroy ? 8 : 0);
     int st;
-    if (o->dim == 2) st = build_2d(o);
-    else if (o->dim == 3) st = build_3d(o);
-    else st = build_4d(o);
-    if (st == FFTB_SUCCESS && o->dim == 3) st = fused3d_init(o->fused, dtype, nx, ny, nz);
-    if (st == FFTB_SUCCESS && o->dim == 4) st = fused4d_init(o->fused4, dtype, layout4d, nx, ny, nz, nw);
+    {
+        FFTB_PROFILE_SCOPE(o, "init");
+        if (o->dim == 2) st = build_2d(o);
+        else if (o->dim == 3) st = build_3d(o);
+        else st = build_4d(o);
+        if (st == FFTB_SUCCESS && o->dim == 3) st = fused3d_init(o->fused, dtype, nx, ny, nz);
+        if (st == FFTB_SUCCESS && o->dim == 4) st = fused4d_init(o->fused4, dtype, layout4d, nx, ny, nz, nw);
+    }
     if (st != FFTB_SUCCESS) {
+        o->prof.clear_events();
         delete o;
         return st;
     }
@@ -487,10 +542,35 @@ int fftb_ffts_create(int dtype, long long nx, long long ny, long long nz, long l
 int fftb_ffts_destroy(fftb_ffts o)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    // print-on-destroy of the profiles (source/ffts.hpp:199-208, :449-476)
+    if (o->prof.enabled && (o->print_flags & 1)) std::fputs(o->prof.summary().c_str(), stdout);
+    if (o->prof.enabled && (o->print_flags & 2)) std::fputs(o->prof.totals().c_str(), stdout);
+    if (o->mem.enabled && (o->print_flags & 4)) std::fputs(o->mem.summary().c_str(), stdout);
+    if (o->mem.enabled && (o->print_flags & 8)) std::fputs(o->mem.totals().c_str(), stdout);
+    if (o->print_flags) std::fflush(stdout);
+    o->prof.clear_events();
     if (o->own_work && o->work) cudaFree(o->work);
     if (o->dspec) cudaFree(o->dspec);
     if (o->dspec2) cudaFree(o->dspec2);
     delete o;
+    return FFTB_SUCCESS;
+}
+
+int fftb_ffts_profile_report(fftb_ffts o, int which, char *text, size_t capacity, size_t *needed)
+{
+    if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    if (which < 0 || which > 3) return FFTB_ERROR_INVALID_VALUE;
+    std::string r;
+    if (which == 0) r = o->prof.enabled ? o->prof.summary() : std::string();
+    else if (which == 1) r = o->prof.enabled ? o->prof.totals() : std::string();
+    else if (which == 2) r = o->mem.enabled ? o->mem.summary() : std::string();
+    else r = o->mem.enabled ? o->mem.totals() : std::string();
+    if (needed) *needed = r.size() + 1;
+    if (text && capacity > 0) {
+        const size_t n = r.size() < capacity - 1 ? r.size() : capacity - 1;
+        std::memcpy(text, r.data(), n);
+        text[n] = 0;
+    }
     return FFTB_SUCCESS;
 }
 
@@ -515,6 +595,7 @@ int fftb_ffts_set_work_area(fftb_ffts o, void *work)
     if (o->own_work && o->work) cudaFree(o->work);
     o->own_work = false;
     o->work = work;
+    o->mem.set_bytes("ffts/shared_work_buffer", 0);  // an external work area is the caller's
     return FFTB_SUCCESS;
 }
 
@@ -528,6 +609,7 @@ int fftb_ffts_set_stream(fftb_ffts o, void *stream)
 int fftb_ffts_forward(fftb_ffts o, const void *in, void *out)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    FFTB_PROFILE_SCOPE(o, "forward");
     if (!in || !out) return FFTB_ERROR_INVALID_VALUE;
     LaunchTimer *tm = o->timing ? &o->timer : nullptr;
     if (o->fused.enabled && aligned16(in, out)) return fused3d_forward(o->fused, in, out, o->stream, tm);
@@ -542,6 +624,7 @@ int fftb_ffts_forward(fftb_ffts o, const void *in, void *out)
 int fftb_ffts_backward(fftb_ffts o, void *in, void *out)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    FFTB_PROFILE_SCOPE(o, "backward");
     if (!in || !out) return FFTB_ERROR_INVALID_VALUE;
     LaunchTimer *tm = o->timing ? &o->timer : nullptr;
     if (o->fused.enabled && aligned16(in, out)) return fused3d_backward(o->fused, in, out, 1.0, o->stream, tm);
@@ -556,6 +639,7 @@ int fftb_ffts_backward(fftb_ffts o, void *in, void *out)
 int fftb_ffts_backward_normalized(fftb_ffts o, void *in, void *out)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    FFTB_PROFILE_SCOPE(o, "backward_normalized");
     if (!in || !out) return FFTB_ERROR_INVALID_VALUE;
     LaunchTimer *tm = o->timing ? &o->timer : nullptr;
     if (o->fused.enabled && aligned16(in, out))
@@ -572,6 +656,7 @@ int fftb_ffts_backward_normalized(fftb_ffts o, void *in, void *out)
 int fftb_ffts_poisson(fftb_ffts o, const void *rhs, void *sol, double sign)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    FFTB_PROFILE_SCOPE(o, "poisson");
     if (!rhs || !sol) return FFTB_ERROR_INVALID_VALUE;
     EpValues ep;
     ep.scale = 1.0;
@@ -590,6 +675,7 @@ int fftb_ffts_poisson(fftb_ffts o, const void *rhs, void *sol, double sign)
 int fftb_ffts_filter(fftb_ffts o, const void *in, void *out, double sigma, double poisson_sign)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    FFTB_PROFILE_SCOPE(o, "filter");
     if (!in || !out || !(sigma > 0.0)) return FFTB_ERROR_INVALID_VALUE;
     EpValues ep;
     ep.scale = 1.0;
@@ -609,6 +695,7 @@ int fftb_ffts_filter(fftb_ffts o, const void *in, void *out, double sigma, doubl
 int fftb_ffts_forward_adjoint(fftb_ffts o, void *grad_spectrum, void *grad_real)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    FFTB_PROFILE_SCOPE(o, "forward_adjoint");
     if (!grad_spectrum || !grad_real) return FFTB_ERROR_INVALID_VALUE;
     LaunchTimer *tm = o->timing ? &o->timer : nullptr;
     if (o->fused.enabled && aligned16(grad_spectrum, grad_real))
@@ -624,6 +711,7 @@ int fftb_ffts_forward_adjoint(fftb_ffts o, void *grad_spectrum, void *grad_real)
 int fftb_ffts_backward_adjoint(fftb_ffts o, const void *grad_real, void *grad_spectrum)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    FFTB_PROFILE_SCOPE(o, "backward_adjoint");
     if (!grad_spectrum || !grad_real) return FFTB_ERROR_INVALID_VALUE;
     LaunchTimer *tm = o->timing ? &o->timer : nullptr;
     if (o->fused.enabled && aligned16(grad_spectrum, grad_real))
@@ -708,6 +796,8 @@ int ensure_spectrum(fftb_ffts_s *o, void **buf)
         *buf = nullptr;
         return FFTB_ERROR_ALLOC;
     }
+    o->dspec_bytes = bytes;
+    o->mem.set_bytes(buf == &o->dspec ? "ffts/derivative_spectrum" : "ffts/gradient_spectrum", (long long)bytes);
     return FFTB_SUCCESS;
 }
 
@@ -725,6 +815,7 @@ extern "C" {
 int fftb_ffts_derivative(fftb_ffts o, const void *in, void *out, int axis)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    FFTB_PROFILE_SCOPE(o, "derivative");
     if (!in || !out || axis < 0 || axis >= o->dim) return FFTB_ERROR_INVALID_VALUE;
     int st = ensure_spectrum(o, &o->dspec);
     if (st != FFTB_SUCCESS) return st;
@@ -739,6 +830,7 @@ int fftb_ffts_derivative(fftb_ffts o, const void *in, void *out, int axis)
 int fftb_ffts_gradient(fftb_ffts o, const void *in, void *const *outs)
 {
     if (!o) return FFTB_ERROR_INVALID_HANDLE;
+    FFTB_PROFILE_SCOPE(o, "gradient");
     if (!in || !outs) return FFTB_ERROR_INVALID_VALUE;
     for (int a = 0; a < o->dim; ++a)
         if (!outs[a]) return FFTB_ERROR_INVALID_VALUE;

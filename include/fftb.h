@@ -108,11 +108,38 @@ int fftb_plan_destroy(fftb_plan plan);
 /* ------------------------------------------------------------------ ffts transforms */
 typedef struct fftb_ffts_s *fftb_ffts;
 
+/* Profiling options of an ffts object: the reference's ffts_init_options
+ * (source/ffts.hpp:64-72).  A key that is NULL or empty turns that profiler off.  The
+ * profiler records, per API call scope ("ffts::forward<3>" ...), calls, host milliseconds and
+ * device milliseconds (events on the object's stream; skipped while it is being captured);
+ * the memory profiler records the object's own device allocations (work area, derivative
+ * spectra) with their peaks.  The print flags print the reports to stdout when the object is
+ * destroyed (source/ffts.hpp:199-208). */
+typedef struct fftb_init_options {
+    const char *profiling_key;
+    const char *memory_profiling_key;
+    int print_profile_summary_on_destroy;
+    int print_profile_totals_on_destroy;
+    int print_memory_profile_on_destroy;
+    int print_memory_totals_on_destroy;
+} fftb_init_options;
+
+/* The reference's defaults: keys "ffts_prof" / "ffts_mem", every print on. */
+void fftb_init_options_default(fftb_init_options *options);
+
 /* ffts() + ffts::init(nx, ny[, nz[, nw]]) (source/ffts.hpp:192-285).  layout4d is
  * one of FFTB_4D_* and ignored for 2D/3D.  nz = nw = 0 selects 2D; nw = 0 3D. */
 int fftb_ffts_create(int dtype, long long nx, long long ny, long long nz, long long nw, int layout4d,
                      fftb_ffts *obj);
+/* fftb_ffts_create with profiling options (NULL: fftb_init_options_default); fftb_ffts_create
+ * itself has both profilers off. */
+int fftb_ffts_create_ex(int dtype, long long nx, long long ny, long long nz, long long nw, int layout4d,
+                        const fftb_init_options *options, fftb_ffts *obj);
 int fftb_ffts_destroy(fftb_ffts obj);
+/* One report of the object's profilers as text (which: 0 profile summary, 1 profile totals,
+ * 2 memory profile, 3 memory totals; empty when that profiler is off).  *needed receives the
+ * size with the terminating zero; text is truncated to capacity. */
+int fftb_ffts_profile_report(fftb_ffts obj, int which, char *text, size_t capacity, size_t *needed);
 /* ffts::dimension (source/ffts.hpp:330-334) */
 int fftb_ffts_dimension(fftb_ffts obj, int *dim);
 /* Work bytes the object needs for forward/backward/poisson (the reference's shared
@@ -282,6 +309,9 @@ int fftb_autotune_save_file(const char *path, const char *text);
  * expected_text are compared; the cache must also be a measured fftb cache).  Returns
  * FFTB_ERROR_CACHE_MISMATCH with a message naming the first differing key. */
 int fftb_autotune_validate(const char *cache_text, const char *expected_text, int flags);
+/* "v2:" + 64-bit FNV-1a (16 hex digits) of a canonical hardware description: the hash the
+ * reference's hardware signatures use (source/detail/fftm_autotune_hardware.inc:87-97). */
+int fftb_autotune_signature(const char *canonical, char *text, size_t capacity, size_t *needed);
 /* The hardware keys (signatures and device metadata) of a CUDA device. */
 int fftb_autotune_hardware(int device, char *text, size_t capacity, size_t *needed);
 /* load_or_measure for an ffts problem (dims and layout4d as fftb_ffts_create) on the

@@ -54,6 +54,92 @@ enum class strategy_4d : int {
     native_xzwy = FFTB_4D_NATIVE_XZWY
 };
 
+/* ffts_init_options (source/ffts.hpp:64-72): both profilers on and every report printed
+ * when the object is destroyed, unless a key is emptied or a flag cleared. */
+struct ffts_init_options {
+    std::string profiling_key = "ffts_prof";
+    std::string memory_profiling_key = "ffts_mem";
+    bool print_profile_summary_on_destroy = true;
+    bool print_profile_totals_on_destroy = true;
+    bool print_memory_profile_on_destroy = true;
+    bool print_memory_totals_on_destroy = true;
+};
+
+/* fftm_reporting_options (source/fftm_options.hpp:220-229) and the profiling preset
+ * (:231-242); on one GPU the fftm frontend's path is this ffts, so they map onto
+ * ffts_init_options. */
+struct fftm_reporting_options {
+    std::string profiling_key;
+    std::string memory_profiling_key;
+    bool verbose = false;
+    bool print_profile_summary_on_destroy = false;
+    bool print_profile_totals_on_destroy = false;
+    bool print_memory_profile_on_destroy = false;
+    bool print_memory_totals_on_destroy = false;
+};
+inline fftm_reporting_options profiling_reporting_options()
+{
+    fftm_reporting_options o;
+    o.profiling_key = "fftm_prof";
+    o.memory_profiling_key = "fftm_mem";
+    o.print_profile_summary_on_destroy = true;
+    o.print_profile_totals_on_destroy = true;
+    o.print_memory_profile_on_destroy = true;
+    o.print_memory_totals_on_destroy = true;
+    return o;
+}
+inline ffts_init_options to_ffts_init_options(const fftm_reporting_options &r)
+{
+    ffts_init_options o;
+    o.profiling_key = r.profiling_key;
+    o.memory_profiling_key = r.memory_profiling_key;
+    o.print_profile_summary_on_destroy = r.print_profile_summary_on_destroy;
+    o.print_profile_totals_on_destroy = r.print_profile_totals_on_destroy;
+    o.print_memory_profile_on_destroy = r.print_memory_profile_on_destroy;
+    o.print_memory_totals_on_destroy = r.print_memory_totals_on_destroy;
+    return o;
+}
+
+/* fftm_4d_spectral_layout (source/fftm_options.hpp:48-52) and the single-GPU part of
+ * fftm_init_options (:347-357): public_yzwx is the ffts pencil spectrum [ky][kz][kw][kx]
+ * (byte-identical), native_xzwy fftm's slab path with the same spectrum order. */
+enum class fftm_4d_spectral_layout { public_yzwx, native_xzwy };
+struct fftm_init_options {
+    bool use_optimized = true;
+    fftm_4d_spectral_layout spectral_layout_4d = fftm_4d_spectral_layout::public_yzwx;
+    fftm_reporting_options reporting;
+};
+inline strategy_4d strategy_for(fftm_4d_spectral_layout l)
+{
+    return l == fftm_4d_spectral_layout::native_xzwy ? strategy_4d::native_xzwy : strategy_4d::pencil_pencil;
+}
+
+/* A named byte counter with peaks: the memory profiler fft_wrap_many::set_memory_profiler
+ * reports into (the role of the reference's memory_profiler_t). */
+class memory_profiler {
+public:
+    using bytes_type = long long;
+    struct entry {
+        bytes_type current_bytes = 0, peak_bytes = 0;
+    };
+    void set_bytes(const std::string &name, bytes_type b)
+    {
+        entry &e = entries_[name];
+        e.current_bytes = b;
+        if (b > e.peak_bytes) e.peak_bytes = b;
+    }
+    const std::map<std::string, entry> &entries() const { return entries_; }
+    bytes_type total_current() const
+    {
+        bytes_type t = 0;
+        for (const auto &kv : entries_) t += kv.second.current_bytes;
+        return t;
+    }
+
+private:
+    std::map<std::string, entry> entries_;
+};
+
 /* A library failure: the status code and the library's message. */
 class error : public std::runtime_error {
 public:
@@ -280,6 +366,7 @@ public:
             for (auto &el : container_) el.second->set_work_area(work_area_);
         }
         activated_ = true;
+        update_memory_profile_();
     }
     void set_external_work_area(void *w)
     {
@@ -287,8 +374,18 @@ public:
             throw std::logic_error("fft_wrap_many::set_external_work_area: cannot set external work_area with "
                                    "activated local work_area.");
         for (auto &el : container_) el.second->set_work_area(w);
+        external_activated_ = true;
+        update_memory_profile_();
     }
     std::size_t get_work_size() const { return work_area_size_; }
+    /* reports "<prefix>/work_area" (the bytes this object allocated; 0 with an external work
+     * area) to `profiler`, now and whenever it changes (source/external_wrap/fft_wrap_many.h:298-303) */
+    void set_memory_profiler(memory_profiler *profiler, const std::string &prefix)
+    {
+        memory_profiler_ = profiler;
+        memory_profile_prefix_ = prefix;
+        update_memory_profile_();
+    }
     void set_stream(cudaStream_t s)
     {
         for (auto &el : container_) el.second->set_stream(s);
@@ -321,11 +418,24 @@ private:
         work_area_ = nullptr;
         work_area_size_ = 0;
         activated_ = false;
+        try {
+            update_memory_profile_();
+        } catch (...) {
+        }
+    }
+    void update_memory_profile_()
+    {
+        if (!memory_profiler_ || memory_profile_prefix_.empty()) return;
+        memory_profiler_->set_bytes(memory_profile_prefix_ + "/work_area",
+                                    external_activated_ ? 0 : (memory_profiler::bytes_type)work_area_size_);
     }
     std::map<std::string, std::unique_ptr<wrap_t>> container_;
     std::size_t work_area_size_ = 0;
     void *work_area_ = nullptr;
     bool activated_ = false;
+    bool external_activated_ = false;
+    memory_profiler *memory_profiler_ = nullptr;
+    std::string memory_profile_prefix_;
 };
 
 /* ====================================================================== autotune */
@@ -458,9 +568,35 @@ public:
         if (h_) fftb_ffts_destroy(h_);
     }
 
-    void init(long long nx, long long ny) { init_(nx, ny, 0, 0); }
-    void init(long long nx, long long ny, long long nz) { init_(nx, ny, nz, 0); }
-    void init(long long nx, long long ny, long long nz, long long nw) { init_(nx, ny, nz, nw); }
+    /* init with the reference's overloads (source/ffts.hpp:227-285): the default options turn
+     * both profilers on and print their reports when the object is destroyed */
+    void init(long long nx, long long ny, const ffts_init_options &o = ffts_init_options()) { init_(nx, ny, 0, 0, o); }
+    void init(long long nx, long long ny, long long nz, const ffts_init_options &o = ffts_init_options())
+    {
+        init_(nx, ny, nz, 0, o);
+    }
+    void init(long long nx, long long ny, long long nz, long long nw, const ffts_init_options &o = ffts_init_options())
+    {
+        init_(nx, ny, nz, nw, o);
+    }
+    template <std::size_t Dim>
+    void init(const std::array<std::size_t, Dim> &grid, const ffts_init_options &o = ffts_init_options())
+    {
+        static_assert(Dim >= 2 && Dim <= 4, "ffts: 2D, 3D or 4D");
+        init_((long long)grid[0], (long long)grid[1], Dim > 2 ? (long long)grid[Dim > 2 ? 2 : 0] : 0,
+              Dim > 3 ? (long long)grid[Dim > 3 ? 3 : 0] : 0, o);
+    }
+    /* one report of the profilers as text: 0 profile summary, 1 totals, 2 memory, 3 memory totals */
+    std::string profile_report(int which = 0) const
+    {
+        ensure_initialized_();
+        size_t need = 0;
+        check(fftb_ffts_profile_report(h_, which, nullptr, 0, &need), "ffts::profile_report");
+        std::string t(need, '\0');
+        check(fftb_ffts_profile_report(h_, which, &t[0], t.size(), &need), "ffts::profile_report");
+        t.resize(need ? need - 1 : 0);
+        return t;
+    }
 
     bool is_initialized() const { return h_ != nullptr; }
     std::size_t dimension() const
@@ -614,10 +750,18 @@ public:
     fftb_ffts handle() const { return h_; }
 
 private:
-    void init_(long long nx, long long ny, long long nz, long long nw)
+    void init_(long long nx, long long ny, long long nz, long long nw, const ffts_init_options &o)
     {
         if (h_) throw std::logic_error("ffts::init can only be called once per instance.");
-        check(fftb_ffts_create(detail::dtype_code<T>::value, nx, ny, nz, nw, static_cast<int>(S), &h_), "ffts::init");
+        fftb_init_options c;
+        c.profiling_key = o.profiling_key.c_str();
+        c.memory_profiling_key = o.memory_profiling_key.c_str();
+        c.print_profile_summary_on_destroy = o.print_profile_summary_on_destroy ? 1 : 0;
+        c.print_profile_totals_on_destroy = o.print_profile_totals_on_destroy ? 1 : 0;
+        c.print_memory_profile_on_destroy = o.print_memory_profile_on_destroy ? 1 : 0;
+        c.print_memory_totals_on_destroy = o.print_memory_totals_on_destroy ? 1 : 0;
+        check(fftb_ffts_create_ex(detail::dtype_code<T>::value, nx, ny, nz, nw, static_cast<int>(S), &c, &h_),
+              "ffts::init");
         n_ = {nx, ny, nz, nw};
         dim_ = nw ? 4 : (nz ? 3 : 2);
     }

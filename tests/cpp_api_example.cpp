@@ -8,7 +8,8 @@
 //      closed-form solutions;
 //   4. ffts<double, native_xzwy> 4D round trip;
 //   5. load_or_measure_config: measured once, then read back from the cache;
-//   6. batch<float>: uneven 3D round trips in one graph-replayed launch.
+//   6. batch<float>: uneven 3D round trips in one graph-replayed launch;
+//   7. the profiling options (ffts_init_options, fftm_reporting_options) and reports.
 // Prints one line per check and "ok" last; exit status 0 when every check passes.
 // argv[1]: a writable directory for the autotune cache, or "--host-only" to run just the
 // checks that need no GPU (status -> exception mapping, KEY=VALUE text, option flags).
@@ -101,6 +102,31 @@ void host_only()
     o.validate_hardware = false;
     expect(o.flags() == (FFTB_TUNE_CREATE_IF_MISSING | FFTB_TUNE_OVERWRITE_ON_MISMATCH | FFTB_TUNE_NO_HARDWARE_CHECK),
            "autotune_options flags");
+    // the reference's option structs and presets (source/ffts.hpp:64-72, source/fftm_options.hpp:220-242)
+    const fftb::ffts_init_options io;
+    expect(io.profiling_key == "ffts_prof" && io.memory_profiling_key == "ffts_mem" &&
+               io.print_profile_summary_on_destroy && io.print_memory_totals_on_destroy,
+           "ffts_init_options defaults");
+    const fftb::fftm_reporting_options quiet;
+    const fftb::ffts_init_options qo = fftb::to_ffts_init_options(quiet);
+    expect(qo.profiling_key.empty() && !qo.print_profile_summary_on_destroy, "fftm_reporting_options defaults off");
+    const fftb::ffts_init_options po = fftb::to_ffts_init_options(fftb::profiling_reporting_options());
+    expect(po.profiling_key == "fftm_prof" && po.memory_profiling_key == "fftm_mem" && po.print_memory_profile_on_destroy,
+           "profiling_reporting_options preset");
+    expect(fftb::strategy_for(fftb::fftm_4d_spectral_layout::native_xzwy) == fftb::strategy_4d::native_xzwy &&
+               fftb::strategy_for(fftb::fftm_4d_spectral_layout::public_yzwx) == fftb::strategy_4d::pencil_pencil,
+           "fftm spectral layout -> ffts strategy");
+    // memory profiler attached to a plan registry (source/external_wrap/fft_wrap_many.h:298-303)
+    fftb::memory_profiler mp;
+    mp.set_bytes("a", 100);
+    mp.set_bytes("a", 40);
+    expect(mp.entries().at("a").current_bytes == 40 && mp.entries().at("a").peak_bytes == 100, "memory profiler peaks");
+    fftb::fft_wrap_many<float> reg;
+    reg.set_memory_profiler(&mp, "ffts/base_fft");
+    reg.activate();
+    expect(mp.entries().count("ffts/base_fft/work_area") == 1 &&
+               mp.entries().at("ffts/base_fft/work_area").current_bytes == 0,
+           "fft_wrap_many reports its work area to the memory profiler");
 }
 
 void plan_registry()
@@ -163,6 +189,28 @@ void ffts_3d()
     expect(throws_logic([&] { f.init(N, N, N); }), "ffts::init twice -> std::logic_error");
     expect(throws_logic([&] { f.ensure_dimension(4); }), "3D ffts used as 4D -> std::logic_error");
     expect(f.dimension() == 3 && f.spectrum_size() == (long long)N * N * (N / 2 + 1), "ffts sizes");
+    {
+        // profilers with their reports read back instead of printed
+        fftb::ffts_init_options po;
+        po.profiling_key = "p3";
+        po.memory_profiling_key = "m3";
+        po.print_profile_summary_on_destroy = po.print_profile_totals_on_destroy = false;
+        po.print_memory_profile_on_destroy = po.print_memory_totals_on_destroy = false;
+        fftb::ffts<float> g;
+        g.init(std::array<std::size_t, 3>{(std::size_t)N, (std::size_t)N, (std::size_t)N}, po);
+        device_array<float> a(n), b(n);
+        cudaMemset(a.raw_ptr(), 0, n * sizeof(float));
+        g.poisson(a, b, -1.0);
+        g.poisson(a, b, -1.0);
+        cudaDeviceSynchronize();
+        const std::string rep = g.profile_report(0), mem = g.profile_report(2);
+        expect(rep.find("Profile p3:") != std::string::npos && rep.find("ffts::poisson<3>: calls=2") != std::string::npos &&
+                   rep.find("ffts::init<3>: calls=1") != std::string::npos,
+               "ffts profile report (scopes and calls)");
+        expect(mem.find("ffts/shared_work_buffer: current(sum/max/avg)=" + std::to_string(g.work_size())) !=
+                   std::string::npos,
+               "ffts memory profile (the work area it allocated)");
+    }
     std::vector<float> rhs(n);
     std::vector<double> u_exact(n), uy_exact(n);
     for (int x = 0; x < N; ++x)

@@ -92,7 +92,7 @@ def test_validate_accepts_matching_cache(A):
 
 @pytest.mark.parametrize("key,value", [
     ("FFTM_AUTOTUNE_SIZE_3D", "128x128x128"), ("FFTM_AUTOTUNE_SCHEMA", "1"), ("FFTM_AUTOTUNE_DIM", "4"),
-    ("FFTM_AUTOTUNE_LIBRARY", "fftm"), ("FFTB_AUTOTUNE_DTYPE", "float64"), ("FFTM_AUTOTUNE_NUM_GPUS", "2"),
+    ("FFTB_AUTOTUNE_DTYPE", "float64"), ("FFTM_AUTOTUNE_NUM_GPUS", "2"),
     ("FFTM_AUTOTUNE_POLICY_VERSION", "4"),
 ])
 def test_validate_rejects_other_problem(A, key, value):
@@ -104,10 +104,54 @@ def test_validate_rejects_other_problem(A, key, value):
         A.validate(_cache(**{key: value}), IDENT, A.autotune_options(validate_hardware=False))
 
 
-def test_validate_rejects_policy_cache_of_the_reference(A):
-    # a cache the reference's policy wrote (not a measured fftb cache)
+def test_validate_rejects_unmeasured_fftb_cache(A):
+    # an fftb cache must come from a measurement
     with pytest.raises(FftbError, match="not a measured"):
         A.validate(_cache(FFTM_AUTOTUNE_SOURCE="cpp-policy-cache-v4"), IDENT)
+
+
+def _reference_policy_cache(**over):
+    # what the reference's make_default_3d_policy_config writes for one rank
+    # (source/fftm_autotune.hpp:595-605, :660-681) plus its hardware keys
+    c = {"FFTM_AUTOTUNE_SCHEMA": "2", "FFTM_AUTOTUNE_POLICY_VERSION": "4", "FFTM_AUTOTUNE_LIBRARY": "fftm",
+         "FFTM_AUTOTUNE_DIM": "3", "FFTM_AUTOTUNE_NUM_GPUS": "1", "FFTM_AUTOTUNE_SIZE_3D": "256x256x256",
+         "FFTM_AUTOTUNE_SOURCE": "cpp-policy-cache-v4", "FFTM_AUTOTUNE_STRATEGY_3D": "slab-pencil",
+         "FFTM_AUTOTUNE_GRID_3D": "1x1", "FFTM_AUTOTUNE_PENCIL_LAYOUT": "auto",
+         "FFTM_AUTOTUNE_PENCIL_PIPELINE": "staged", "FFTM_AUTOTUNE_HARDWARE_SIGNATURE_VERSION": "2",
+         "FFTM_AUTOTUNE_HARDWARE_SIGNATURE": IDENT["FFTM_AUTOTUNE_HARDWARE_SIGNATURE"],
+         "FFTM_AUTOTUNE_HARDWARE_SIGNATURE_STRICT": IDENT["FFTM_AUTOTUNE_HARDWARE_SIGNATURE_STRICT"]}
+    c.update(over)
+    return c
+
+
+def test_validate_accepts_single_gpu_cache_of_the_reference(A):
+    A.validate(_reference_policy_cache(), IDENT)
+    A.validate(_reference_policy_cache(FFTM_AUTOTUNE_STRATEGY_3D="pencil-slab"), IDENT,
+               A.autotune_options(strict_device_identity=True))
+
+
+@pytest.mark.parametrize("key,value", [("FFTM_AUTOTUNE_SIZE_3D", "128x128x128"), ("FFTM_AUTOTUNE_NUM_GPUS", "4"),
+                                       ("FFTM_AUTOTUNE_SCHEMA", "1"), ("FFTM_AUTOTUNE_DIM", "4"),
+                                       ("FFTM_AUTOTUNE_HARDWARE_SIGNATURE", "v2:1111111111111111")])
+def test_validate_rejects_reference_cache_of_another_problem_or_machine(A, key, value):
+    with pytest.raises(FftbError) as e:
+        A.validate(_reference_policy_cache(**{key: value}), IDENT)
+    assert e.value.status == CACHE_MISMATCH
+
+
+def test_hardware_signature_follows_the_reference_hash(A):
+    # 64-bit FNV-1a of the canonical string, "v2:" + 16 hex digits
+    # (source/detail/fftm_autotune_hardware.inc:87-97)
+    def fnv(s):
+        h = 14695981039346656037
+        for ch in s.encode():
+            h = ((h ^ ch) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+        return f"{h:016x}"
+    assert fnv("") == "cbf29ce484222325"
+    canon = ("version=2;mpi_ranks=1;node_count=1;ranks_per_node=1;devices_per_node=1;mpi_library=unavailable;"
+             "device_classes=backend_cuda:model_NVIDIA_B200:arch_10.0:memory_1:runtime_12090:driver_13000;"
+             "transport=local;transport_env=affinity_default:ucx_tls_default")
+    assert A.signature(canon) == "v2:" + fnv(canon)
 
 
 def test_validate_hardware_signature(A):

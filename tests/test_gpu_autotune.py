@@ -27,8 +27,70 @@ def test_hardware_keys(F):
     assert hw["FFTM_AUTOTUNE_HARDWARE_SIGNATURE"].startswith("v2:")
     assert hw["FFTM_AUTOTUNE_HARDWARE_SIGNATURE_STRICT"].startswith("v2:")
     assert hw["FFTM_AUTOTUNE_HARDWARE_SIGNATURE"] != hw["FFTM_AUTOTUNE_HARDWARE_SIGNATURE_STRICT"]
-    assert hw["FFTM_AUTOTUNE_GPU_ARCHITECTURES"].startswith("sm_")
+    assert hw["FFTM_AUTOTUNE_GPU_ARCHITECTURES"] == "10.0"
     assert A.hardware_config(0) == hw
+
+
+def _token(v):
+    # the reference's normalize_hardware_token (source/detail/fftm_autotune_hardware.inc:28-49)
+    import re
+    t = re.sub(r"[\x00\s;=,|]+", "_", v).strip("_")
+    return t or "unknown"
+
+
+def test_hardware_signature_is_the_reference_canonical_string(F, torch_cuda):
+    # the single-rank canonical compatibility string of
+    # source/detail/fftm_autotune_hardware.inc:285-310, rebuilt here from the device
+    # properties and the environment, must be the one the library hashed
+    torch = torch_cuda
+    import fftm_b200.autotune as A
+    hw = A.hardware_config(0)
+    canon = hw["FFTB_AUTOTUNE_CANONICAL_COMPATIBILITY"]
+    assert A.signature(canon) == hw["FFTM_AUTOTUNE_HARDWARE_SIGNATURE"]
+    p = torch.cuda.get_device_properties(0)
+    fields = dict(f.split("=", 1) for f in canon.split(";"))
+    assert list(fields) == ["version", "mpi_ranks", "node_count", "ranks_per_node", "devices_per_node",
+                            "mpi_library", "device_classes", "transport", "transport_env"]
+    assert (fields["version"], fields["mpi_ranks"], fields["node_count"], fields["ranks_per_node"],
+            fields["devices_per_node"], fields["mpi_library"], fields["transport"]) == \
+        ("2", "1", "1", "1", "1", "unavailable", "local")
+    cls = fields["device_classes"].split(":")
+    assert cls[0] == "backend_cuda" and cls[1] == "model_" + _token(p.name) and cls[2] == f"arch_{p.major}.{p.minor}"
+    assert cls[3] == f"memory_{p.total_memory}" and cls[4].startswith("runtime_") and cls[5].startswith("driver_")
+    env = "affinity={}:ucx_tls={}:ucx_net_devices={}:mpi_pml={}:mpi_btl={}".format(
+        *[_token(os.environ.get(k, "default")) for k in ("FFTM_MPI_RANK_AFFINITY_MODE", "UCX_TLS", "UCX_NET_DEVICES",
+                                                         "OMPI_MCA_pml", "OMPI_MCA_btl")])
+    assert fields["transport_env"] == _token(env)
+
+
+def test_reference_written_single_gpu_cache_is_used(F, torch_cuda, tmp_path):
+    # a cache as the reference's policy writes it for one rank on this machine: used as is
+    # (nothing measured, the file untouched), its decomposition mapped onto the default
+    # execution, and the transform still matches the oracle
+    torch = torch_cuda
+    import fftm_b200.autotune as A
+    hw = A.hardware_config(0)
+    ref = {"FFTM_AUTOTUNE_SCHEMA": "2", "FFTM_AUTOTUNE_POLICY_VERSION": "4", "FFTM_AUTOTUNE_LIBRARY": "fftm",
+           "FFTM_AUTOTUNE_DIM": "3", "FFTM_AUTOTUNE_NUM_GPUS": "1", "FFTM_AUTOTUNE_SIZE_3D": "64x64x64",
+           "FFTM_AUTOTUNE_SOURCE": "cpp-policy-cache-v4", "FFTM_AUTOTUNE_STRATEGY_3D": "slab-pencil",
+           "FFTM_AUTOTUNE_GRID_3D": "1x1", "FFTM_AUTOTUNE_PENCIL_LAYOUT": "auto",
+           "FFTM_AUTOTUNE_PENCIL_PIPELINE": "staged"}
+    for k in ("FFTM_AUTOTUNE_HARDWARE_SIGNATURE_VERSION", "FFTM_AUTOTUNE_HARDWARE_SIGNATURE",
+              "FFTM_AUTOTUNE_HARDWARE_SIGNATURE_STRICT"):
+        ref[k] = hw[k]
+    path = tmp_path / "fftm_autotune_3d.env"
+    A.save_key_value_file(path, ref)
+    mtime = os.path.getmtime(path)
+    f = F.ffts("float32").init(64, 64, 64)
+    sel = f.autotune(path, A.autotune_options(create_if_missing=False, strict_device_identity=True))
+    assert sel.source == "cache" and os.path.getmtime(path) == mtime
+    assert sel.strategy == "auto" and sel.config["FFTB_AUTOTUNE_REFERENCE_STRATEGY_3D"] == "slab-pencil"
+    x = O.random_3d(64, 64, 64, 0x77, single=True)
+    xin = torch.tensor(x, dtype=torch.float32, device="cuda")
+    spec = torch.empty(f.spectrum_shape(), dtype=torch.complex64, device="cuda")
+    f.forward(xin, spec)
+    torch.cuda.synchronize()
+    assert O.rel_l2(spec.cpu().numpy().astype(np.complex128), O.ffts3d_forward(x)) <= 2e-6
 
 
 def test_ffts_cache_life_cycle(F, torch_cuda, tmp_path):
