@@ -889,7 +889,8 @@ int launch_plane_n(const PlaneEntry *e, long long nplanes, bool inverse, const v
 int launch_plane(const Fused3D &f, bool inverse, const void *in, void *out, double scale, cudaStream_t s,
                  LaunchTimer *tm)
 {
-    return launch_plane_n((const PlaneEntry *)f.plane, f.nx, inverse, in, out, f.roots_plane, scale, s, tm);
+    return launch_plane_n((const PlaneEntry *)(inverse ? f.plane_inv : f.plane), f.nx, inverse, in, out,
+                          f.roots_plane, scale, s, tm);
 }
 
 XColEp make_ep(const EpValues *ep)
@@ -1050,9 +1051,23 @@ int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz
     }
     const XColEntry *xe = find_xcol(dtype, (int)nx);
     if (!pe || !xe) return FFTB_SUCCESS;
+    // The inverse plane kernel is a launch of its own, so it may use another cluster size:
+    // unless one was forced, the smallest cluster (up to 4) whose inverse CTAs fit two per SM,
+    // when the forward's cluster leaves one per SM.  Measured on B200 at 256x256 planes: the
+    // inverse runs 67 us with 4-CTA clusters (two quarter planes per SM) against 71 us with
+    // 2-CTA clusters, while the forward is fastest with 2 (56 against 60 us).
+    const PlaneEntry *pi = pe;
+    if (force_cluster <= 0 && 2 * pe->smem_inv > 227 * 1024)
+        for (int cl = pe->cl * 2; cl <= 4; cl *= 2) {
+            const PlaneEntry *e = find_plane(dtype, (int)ny, (int)nz, cl);
+            if (e && 2 * e->smem_inv <= 227 * 1024) {
+                pi = e;
+                break;
+            }
+        }
     int st;
     if ((st = configure(pe->fwd, pe->smem_fwd)) != FFTB_SUCCESS) return st;
-    if ((st = configure(pe->inv, pe->smem_inv)) != FFTB_SUCCESS) return st;
+    if ((st = configure(pi->inv, pi->smem_inv)) != FFTB_SUCCESS) return st;
     for (int m = 0; m < 5; ++m)
         if ((st = configure(xe->fn[m], xe->smem)) != FFTB_SUCCESS ||
             (st = configure(xe->fn_tc[m], xe->smem_tc)) != FFTB_SUCCESS ||
@@ -1062,8 +1077,10 @@ int fused3d_init(Fused3D &f, int dtype, long long nx, long long ny, long long nz
     if ((st = engine_roots(dtype, nmax, &f.roots_plane)) != FFTB_SUCCESS) return st;
     if ((st = engine_roots(dtype, (int)nx, &f.roots_x)) != FFTB_SUCCESS) return st;
     f.plane = pe;
+    f.plane_inv = pi;
     f.xcol = xe;
     f.cluster = pe->cl;
+    f.cluster_inv = pi->cl;
     f.enabled = true;
     return FFTB_SUCCESS;
 }

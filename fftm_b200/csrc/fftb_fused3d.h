@@ -12,9 +12,11 @@ struct Fused3D {
     bool enabled = false;
     int dtype = 0;
     long long nx = 0, ny = 0, nz = 0;
-    int cluster = 0;               // CTAs per (y, z) plane of the selected plane kernels
+    int cluster = 0;               // CTAs per (y, z) plane of the forward plane kernel
+    int cluster_inv = 0;           // the same for the inverse plane kernel (may differ)
     bool tc = false;               // column kernels with the first radix-16 stage on the tensor cores
-    const void *plane = nullptr;   // selected plane kernel entry
+    const void *plane = nullptr;   // selected plane kernel entry (forward)
+    const void *plane_inv = nullptr;  // entry whose inverse kernel runs (its own cluster size)
     const void *xcol = nullptr;    // selected x column kernel entry
     void *roots_plane = nullptr;   // device root table of length max(ny, nz)
     void *roots_x = nullptr;       // device root table of length nx
