@@ -1,6 +1,7 @@
 // fftb_engine.cu -- kernel registry, twiddle tables, program builder / executor.
 #include "fftb_engine.h"
 #include "fftb_bluestein.h"
+#include "fftb_longline.h"
 
 #include <algorithm>
 #include <cstring>
@@ -175,8 +176,29 @@ int program_add(Program &prog, int dtype, const AxisPass &p)
         a.bs_chirp = ch;
         a.bs_bhat = bh;
     } else {
-        set_last_error("no kernel for line length " + std::to_string(p.n));
-        return FFTB_ERROR_UNSUPPORTED_SIZE;
+        // longer than one pass kernel holds: a long-line step (four-step or chirp-z)
+        std::shared_ptr<LongLine> ll;
+        int st = longline_create(dtype, p, ll);
+        if (st != FFTB_SUCCESS) return st;
+        Launch S;
+        memset(&S.args, 0, sizeof(S.args));
+        S.in_buf = p.in_buf;
+        S.out_buf = p.out_buf;
+        S.in_off_bytes = S.out_off_bytes = 0;
+        S.pair_candidate = 0;
+        S.real_align = 0;
+        S.real_side = 0;
+        S.block = 0;
+        S.smem = 0;
+        S.ep_dynamic = p.ep_dynamic;
+        S.alg_bytes = longline_alg_bytes(*ll);
+        static const char *kn[] = {"c2c_fwd", "c2c_inv", "r2c", "c2r", "sandwich"};
+        S.name = std::string("fftb_long_line<") + (dtype == 0 ? "f32" : "f64") + ">/" + kn[p.kind] + "/n" +
+                 std::to_string(p.n);
+        S.longline = ll;
+        prog.dtype = dtype;
+        prog.launches.push_back(S);
+        return FFTB_SUCCESS;
     }
     const int ntw = chirpz ? L.k.nf : (half ? 2 * nf : nf);
     void *roots = nullptr;
@@ -210,6 +232,7 @@ int program_add(Program &prog, int dtype, const AxisPass &p)
                      (labs_ll(b[0].os) != 1 && labs_ll(p.os) < labs_ll(b[0].os));
     a.tw = roots;
     a.ntw = ntw;
+    a.ep_tw = p.ep_tw;
     const size_t cb = complex_bytes(dtype);
     a.tw_smem = ((size_t)ntw * cb <= 16384) ? 1 : 0;
 
@@ -368,6 +391,11 @@ int program_exec(const Program &prog, void *in, void *out, void *work, cudaStrea
         if (timer) {
             int ts = timer_mark(timer, stream, L.name, L.alg_bytes);
             if (ts != FFTB_SUCCESS) return ts;
+        }
+        if (L.longline) {
+            int st = longline_exec(*L.longline, bufs, stream, ep && L.ep_dynamic ? ep : nullptr);
+            if (st != FFTB_SUCCESS) return st;
+            continue;
         }
         PassArgs a = L.args;
         char *ib = (char *)bufs[L.in_buf];

@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -45,7 +46,10 @@ struct AxisPass {
     double ep_scale = 1.0, ep_sign = -1.0, ep_gauss = 0.0, ep_hw = 1.0;
     std::vector<EpAxis> ep_axes;
     int ep_dynamic = 0;         // epilogue parameters supplied at execution
+    const void *ep_tw = nullptr;  // EP_TWIDDLE root table
 };
+
+struct LongLine;
 
 struct Launch {
     PassArgs args;
@@ -61,6 +65,7 @@ struct Launch {
     int ep_dynamic;
     std::string name;   // kernel + geometry, for timing reports
     double alg_bytes;   // bytes the launch must read and write once (its algorithmic traffic)
+    std::shared_ptr<LongLine> longline;  // set: a long-line step (fftb_longline.cu) instead of one pass
 };
 
 struct Program {

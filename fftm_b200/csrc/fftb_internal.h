@@ -23,6 +23,8 @@ enum EpMode : int {
     EP_GAUSS = 4,    // multiply by exp(-|k|^2 * ep_gauss)
     EP_HALFW = 8,    // multiply interior bins of the half (R2C) axis by ep_hw (adjoint weights)
     EP_DERIV = 16,   // multiply by i k_axis * scale (spectral derivative; fused column kernel)
+    EP_TWIDDLE = 32, // multiply output point p by w_L^(p j), j the batch index of ep_src[0], L = ep_n[0]
+                     // (the inter-step twiddle of a four-step long line; w from the table ep_tw)
 };
 
 // Everything one pass launch needs.  POD, passed by value.
@@ -50,6 +52,7 @@ struct PassArgs {
     int ep_half[4];
     double ep_kscale[4];
     double ep_scale, ep_sign, ep_gauss, ep_hw;
+    const void *ep_tw;        // EP_TWIDDLE: forward roots exp(-2 pi i m / L), m in [0, L)
     // chirp-z passes (bs_n > 0): line length n, chirp table (n) and convolution
     // kernel spectrum (M); tw / ntw are then the roots of the convolution length M
     int bs_n;

@@ -294,6 +294,9 @@ __device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, un
         C *out = reinterpret_cast<C *>(a.out);
         const int nout = (kind == K_R2C) ? (a.half ? NF + 1 : NF / 2 + 1) : NF;
         const int tot = G * nout;
+        const bool twid = (a.ep_mode & EP_TWIDDLE) != 0;
+        const bool fct = ep_store && (a.ep_mode & ~EP_TWIDDLE) != 0;
+        const C *eptw = reinterpret_cast<const C *>(a.ep_tw);
 #pragma unroll 4
         for (int e = tid; e < tot; e += blockDim.x) {
             int gg, p;
@@ -301,7 +304,12 @@ __device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, un
             else { gg = e & (G - 1); p = e >> gshift; }
             if (!bidx[4 * gg + 3]) continue;
             C v = lines[gg * LP + pad16(p)];
-            if (ep_store) v = cscale(v, ep_factor<R>(a, p, bidx + 4 * gg));
+            if (twid) {
+                // p < L1 and j < L2, so p * j < L: no reduction needed
+                const C w = eptw[(long long)p * bidx[4 * gg + a.ep_src[0] - 1]];
+                v = kind == K_C2C_INV ? cmulc(v, w) : cmul(v, w);
+            }
+            if (fct) v = cscale(v, ep_factor<R>(a, p, bidx + 4 * gg));
             out[offs[2 * gg + 1] + p * os] = v;
         }
     }

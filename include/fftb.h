@@ -79,7 +79,12 @@ typedef struct fftb_plan_s *fftb_plan;
 /* Replaces cufft::fft<T,D>::fft(n, inembed, istride, idist, onembed, ostride, odist,
  * batch) -> create_plan -> cufftMakePlanMany64 (source/external_wrap/cufft_wrap.h:533-566,
  * :1237-1259).  inembed/onembed may be NULL for the default tight layout
- * (cufft_wrap.h:568-587).  *work_bytes receives the work-area size (may be 0). */
+ * (cufft_wrap.h:568-587).  *work_bytes receives the work-area size (may be 0).
+ * Line lengths: any length up to 4096 runs one pass kernel per axis (radix passes, or
+ * chirp-z for a large prime factor); longer lines (up to 2^24 points, or 2^21 when a
+ * prime factor above 4096 needs chirp-z) run a long-line step -- four-step through two
+ * pass kernels, or chirp-z over a power-of-two four-step convolution -- that keeps two
+ * work lines of its own (lines x length complex values each) for the plan's lifetime. */
 int fftb_plan_create(int direction, int dtype, int rank, const long long *n, const long long *inembed,
                      long long istride, long long idist, const long long *onembed, long long ostride,
                      long long odist, long long batch, fftb_plan *plan, size_t *work_bytes);
