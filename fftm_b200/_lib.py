@@ -28,6 +28,8 @@ EXPORTS = [
     "fftb_ffts_set_strategy", "fftb_ffts_get_strategy",
     "fftb_autotune_load_file", "fftb_autotune_save_file", "fftb_autotune_validate", "fftb_autotune_hardware", "fftb_autotune_signature",
     "fftb_autotune_ffts", "fftb_ffts_apply_config", "fftb_autotune_batch", "fftb_batch_apply_config",
+    "fftb_slab_create", "fftb_slab_destroy", "fftb_slab_sizes", "fftb_slab_set_stream", "fftb_slab_set_peers",
+    "fftb_slab_forward_local", "fftb_slab_forward_finish", "fftb_slab_backward_local", "fftb_slab_backward_finish",
     "fftb_ffts_spectrum_derivative", "fftb_ffts_derivative", "fftb_ffts_spectrum_truncate", "fftb_ffts_gradient",
 ]
 
@@ -115,6 +117,15 @@ def load():
     L.fftb_ffts_spectrum_truncate.argtypes = [c_vp, c_vp, c_int, c_int]
     L.fftb_ffts_gradient.argtypes = [c_vp, c_vp, ctypes.POINTER(c_vp)]
     L.fftb_batch_set_wait_limit.argtypes = [c_vp, c_ll]
+    L.fftb_slab_create.argtypes = [c_int, c_ll, c_ll, c_ll, c_ll, c_int, c_int, c_int, ctypes.POINTER(c_vp)]
+    L.fftb_slab_destroy.argtypes = [c_vp]
+    L.fftb_slab_sizes.argtypes = [c_vp, llp, llp, llp, llp]
+    L.fftb_slab_set_stream.argtypes = [c_vp, c_vp]
+    L.fftb_slab_set_peers.argtypes = [c_vp, ctypes.POINTER(c_vp)]
+    L.fftb_slab_forward_local.argtypes = [c_vp, c_vp, c_vp, c_vp]
+    L.fftb_slab_forward_finish.argtypes = [c_vp, c_vp, c_vp]
+    L.fftb_slab_backward_local.argtypes = [c_vp, c_vp, c_vp]
+    L.fftb_slab_backward_finish.argtypes = [c_vp, c_vp, c_vp, c_vp]
     L.fftb_batch_wait_selftest.argtypes = [c_ll, ip]
     L.fftb_ffts_create_ex.argtypes = [c_int, c_ll, c_ll, c_ll, c_ll, c_int, ctypes.POINTER(InitOptions),
                                       ctypes.POINTER(c_vp)]

@@ -177,6 +177,10 @@ int program_add(Program &prog, int dtype, const AxisPass &p)
         a.bs_bhat = bh;
     } else {
         // longer than one pass kernel holds: a long-line step (four-step or chirp-z)
+        if (p.in_blk || p.out_blk) {
+            set_last_error("blocked point indices need a C2C pass kernel (line length up to 4096)");
+            return FFTB_ERROR_UNSUPPORTED_SIZE;
+        }
         std::shared_ptr<LongLine> ll;
         int st = longline_create(dtype, p, ll);
         if (st != FFTB_SUCCESS) return st;
@@ -233,6 +237,15 @@ int program_add(Program &prog, int dtype, const AxisPass &p)
     a.tw = roots;
     a.ntw = ntw;
     a.ep_tw = p.ep_tw;
+    if ((p.in_blk || p.out_blk) && (chirpz || (p.kind != K_C2C_FWD && p.kind != K_C2C_INV) ||
+                                    (p.out_blk && p.n / p.out_blk > 8))) {
+        set_last_error("blocked point indices need a C2C pass kernel and at most 8 blocks");
+        return FFTB_ERROR_UNSUPPORTED_SIZE;
+    }
+    a.in_blk = p.in_blk;
+    a.in_hi = p.in_hi;
+    a.out_blk = p.out_blk;
+    a.out_hi = p.out_hi;
     const size_t cb = complex_bytes(dtype);
     a.tw_smem = ((size_t)ntw * cb <= 16384) ? 1 : 0;
 

@@ -47,6 +47,10 @@ struct AxisPass {
     std::vector<EpAxis> ep_axes;
     int ep_dynamic = 0;         // epilogue parameters supplied at execution
     const void *ep_tw = nullptr;  // EP_TWIDDLE root table
+    // blocked point index of a C2C pass (PassArgs in_blk / out_blk): the slab exchanges'
+    // pack (store) and unpack (load); strides in elements
+    int in_blk = 0, out_blk = 0;
+    long long in_hi = 0, out_hi = 0;
 };
 
 struct LongLine;

@@ -57,6 +57,13 @@ struct PassArgs {
     // kernel spectrum (M); tw / ntw are then the roots of the convolution length M
     int bs_n;
     const void *bs_chirp, *bs_bhat;
+    // blocked point index (slab exchanges; C2C passes): in_blk > 0 loads point p from
+    // (p / in_blk) * in_hi + (p % in_blk) * is; out_blk > 0 stores point p at
+    // (p % out_blk) * os from the base of block q = p / out_blk: out_peer[q] when set (a
+    // peer's receive buffer), else out + q * out_hi
+    int in_blk, out_blk;
+    long long in_hi, out_hi;
+    void *out_peer[8];
 };
 
 struct PassKernelInfo {

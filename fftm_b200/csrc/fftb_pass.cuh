@@ -153,7 +153,9 @@ __device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, un
             if (a.in_pts_fast) { gg = e / NF; p = e - gg * NF; }
             else { gg = e & (G - 1); p = e >> gshift; }
             const bool ok = bidx[4 * gg + 3] != 0;
-            stage_load<CG, sizeof(C)>(&lines[gg * LP + pad16(p)], ok ? (const void *)(in + offs[2 * gg] + p * is) : gdummy,
+            const long long pi = a.in_blk ? (long long)(p / a.in_blk) * a.in_hi + (long long)(p % a.in_blk) * is
+                                          : (long long)p * is;
+            stage_load<CG, sizeof(C)>(&lines[gg * LP + pad16(p)], ok ? (const void *)(in + offs[2 * gg] + pi) : gdummy,
                                 ok);
         }
     } else if (kind == K_R2C) {
@@ -310,7 +312,13 @@ __device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, un
                 v = kind == K_C2C_INV ? cmulc(v, w) : cmul(v, w);
             }
             if (fct) v = cscale(v, ep_factor<R>(a, p, bidx + 4 * gg));
-            out[offs[2 * gg + 1] + p * os] = v;
+            if (a.out_blk) {
+                const int q = p / a.out_blk;
+                C *base = a.out_peer[q] ? reinterpret_cast<C *>(a.out_peer[q]) : out + (long long)q * a.out_hi;
+                base[offs[2 * gg + 1] + (long long)(p - q * a.out_blk) * os] = v;
+            } else {
+                out[offs[2 * gg + 1] + p * os] = v;
+            }
         }
     }
 }

@@ -339,6 +339,44 @@ int fftb_autotune_batch(fftb_batch batch, int op, double sign, const char *cache
 /* Applies FFTB_AUTOTUNE_TILES_SCALE / _CTAS_PER_SM of a config; *mode = FFTB_AUTOTUNE_BATCH_MODE. */
 int fftb_batch_apply_config(fftb_batch batch, const char *text, int *mode);
 
+/* ------------------------------------------------------------------ slab-distributed transforms */
+/* The rank-local part of a 3D (x slabs, the reference's slab path with its same_x
+ * redistribution, source/detail/mpi_transpose_3d_same_x.h) or 4D (slab-slab with the
+ * same_xw redistribution, source/detail/mpi_transpose_4d_same_xw.h:437-497) R2C / C2R
+ * distributed over nranks processes, one GPU each.  The pack of the reference's exchange is
+ * the store of the last FFT pass before it and the unpack the load of the first pass after
+ * it, so the exchange is one contiguous block per destination (an all-to-all the caller
+ * runs: NCCL between GPUs), or nothing when the pack pass stores straight into the peers'
+ * receive buffers (fftb_slab_set_peers).
+ *   3D: real slab [nx/P][ny][nz] -> spectrum slab [kx][ny/P][nz/2+1] (rank r: ky block r);
+ *   4D: real slab [nx/P][ny][nz][nw] -> spectrum [kx][ky][nz/P][nw/2+1] (FFTB_4D_SLAB) or
+ *       fftm's native [ky][nz/P][nw/2+1][kx] (FFTB_4D_NATIVE_XZWY), kz block r.
+ * Forward: fftb_slab_forward_local(in -> send) ; exchange send -> recv ;
+ *          fftb_slab_forward_finish(recv -> spectrum: in place on recv, or into out for
+ *          the 4D native layout).  Backward (unnormalised): fftb_slab_backward_local
+ *          (spectrum -> send: in place for 3D) ; exchange ; fftb_slab_backward_finish
+ *          (recv -> real slab).  Exchange blocks are exchange_elems / nranks complex values,
+ *          block q going to rank q and block q of recv coming from rank q.  With one rank,
+ *          send and recv may be the same buffer. */
+typedef struct fftb_slab_s *fftb_slab;
+int fftb_slab_create(int dtype, long long nx, long long ny, long long nz, long long nw, int layout4d, int nranks,
+                     int rank, fftb_slab *obj);
+int fftb_slab_destroy(fftb_slab obj);
+/* elements of the real slab, the spectrum slab, the send / receive buffers (complex) and the
+ * work buffer (complex) */
+int fftb_slab_sizes(fftb_slab obj, long long *real_elems, long long *spectrum_elems, long long *exchange_elems,
+                    long long *work_elems);
+int fftb_slab_set_stream(fftb_slab obj, void *stream);
+/* receive_blocks[q]: where this rank's block lands in rank q's receive buffer, as an address
+ * this GPU can store to (a peer mapping); the forward pack pass then writes there directly
+ * and the caller only synchronises the ranks before forward_finish.  NULL: the pack pass
+ * writes the send buffer. */
+int fftb_slab_set_peers(fftb_slab obj, void *const *receive_blocks);
+int fftb_slab_forward_local(fftb_slab obj, const void *in, void *send, void *work);
+int fftb_slab_forward_finish(fftb_slab obj, void *recv, void *out);
+int fftb_slab_backward_local(fftb_slab obj, void *spectrum, void *send);
+int fftb_slab_backward_finish(fftb_slab obj, void *recv, void *out, void *work);
+
 /* SHA-256 (hex) of the sources the library was compiled from (fftm_b200/csrc and include/),
  * so a caller can check that the library it loaded matches a source tree.  No counterpart in
  * the reference (a header-only library, compiled into its caller). */

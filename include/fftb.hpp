@@ -777,6 +777,56 @@ private:
     std::size_t dim_ = 0;
 };
 
+/* The rank-local part of the slab-distributed 3D / 4D transforms (fftb_slab_*): the pack
+ * pass writes send blocks (or the peers' receive buffers, set_peers), the caller exchanges
+ * block q to rank q (an NCCL all-to-all), the finish passes read the received blocks. */
+template <typename T> class slab {
+public:
+    slab(long long nx, long long ny, long long nz, long long nw, int nranks, int rank,
+         strategy_4d layout = strategy_4d::native_xzwy)
+    {
+        check(fftb_slab_create(detail::dtype_code<T>::value, nx, ny, nz, nw, static_cast<int>(layout), nranks, rank,
+                               &h_),
+              "slab::slab");
+        check(fftb_slab_sizes(h_, &real_, &spec_, &exch_, &work_), "slab::sizes");
+    }
+    slab(const slab &) = delete;
+    slab &operator=(const slab &) = delete;
+    ~slab()
+    {
+        if (h_) fftb_slab_destroy(h_);
+    }
+    long long real_elems() const { return real_; }
+    long long spectrum_elems() const { return spec_; }
+    long long exchange_elems() const { return exch_; }   // complex values of send / receive
+    long long work_elems() const { return work_; }       // complex values of the work buffer
+    void set_stream(cudaStream_t s) { check(fftb_slab_set_stream(h_, (void *)s), "slab::set_stream"); }
+    void set_peers(const std::vector<void *> &receive_blocks)
+    {
+        check(fftb_slab_set_peers(h_, receive_blocks.empty() ? nullptr : receive_blocks.data()), "slab::set_peers");
+    }
+    void forward_local(const void *in, void *send, void *work)
+    {
+        check(fftb_slab_forward_local(h_, in, send, work), "slab::forward_local");
+    }
+    void forward_finish(void *recv, void *out = nullptr)
+    {
+        check(fftb_slab_forward_finish(h_, recv, out), "slab::forward_finish");
+    }
+    void backward_local(void *spectrum, void *send = nullptr)
+    {
+        check(fftb_slab_backward_local(h_, spectrum, send), "slab::backward_local");
+    }
+    void backward_finish(void *recv, void *out, void *work)
+    {
+        check(fftb_slab_backward_finish(h_, recv, out, work), "slab::backward_finish");
+    }
+
+private:
+    fftb_slab h_ = nullptr;
+    long long real_ = 0, spec_ = 0, exch_ = 0, work_ = 0;
+};
+
 /* The allocation-free 3D float32 Poisson solve (fftb_poisson3d_f32_noalloc): static
  * device scratch, spectra up to FFTB_NOALLOC_MAX_SPECTRUM_BYTES, overlapping calls
  * serialised by the caller. */

@@ -236,6 +236,36 @@ void ffts_3d()
     expect(rel_l2(u_na.get(), u_exact) < 1e-5, "poisson3d_noalloc vs the exact solution");
 }
 
+void slab_one_rank()
+{
+    // one rank: the exchange is nothing (send and receive one buffer); the spectrum slab is
+    // then the whole spectrum, equal to ffts' forward
+    const long long nx = 16, ny = 12, nz = 10, n = nx * ny * nz, nc = nx * ny * (nz / 2 + 1);
+    fftb::slab<float> s(nx, ny, nz, 0, 1, 0);
+    expect(s.real_elems() == n && s.spectrum_elems() == nc && s.exchange_elems() == nc, "slab sizes");
+    std::vector<float> h(n);
+    for (long long i = 0; i < n; ++i) h[i] = std::sin(0.37 * (double)i) + 0.01 * (double)(i % 7);
+    device_array<float> x(n);
+    x.put(h);
+    device_array<std::complex<float>> buf(nc), work(s.work_elems()), ref(nc);
+    s.forward_local(x.raw_ptr(), buf.raw_ptr(), work.raw_ptr());
+    s.forward_finish(buf.raw_ptr());
+    fftb::ffts<float> f;
+    fftb::ffts_init_options quiet;
+    quiet.profiling_key.clear();
+    quiet.memory_profiling_key.clear();
+    f.init(nx, ny, nz, quiet);
+    f.forward(x, ref);
+    cudaDeviceSynchronize();
+    const std::vector<std::complex<float>> a = buf.get(), b = ref.get();
+    double num = 0, den = 0;
+    for (long long i = 0; i < nc; ++i) {
+        num += std::norm(std::complex<double>(a[i]) - std::complex<double>(b[i]));
+        den += std::norm(std::complex<double>(b[i]));
+    }
+    expect(std::sqrt(num / den) < 2e-6, "slab<float> one rank equals ffts forward");
+}
+
 void ffts_4d_native()
 {
     const long long nx = 8, ny = 6, nz = 10, nw = 12, n = nx * ny * nz * nw;
@@ -299,6 +329,7 @@ int main(int argc, char **argv)
         plan_registry();
         ffts_3d();
         ffts_4d_native();
+        slab_one_rank();
         autotune(dir);
         batches();
     } catch (const std::exception &e) {

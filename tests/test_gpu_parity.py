@@ -321,10 +321,19 @@ def test_plan_in_place_c2c_and_descriptor(F, torch_cuda):
 
 
 def test_plan_unsupported_size_is_reported(F, torch_cuda):
-    # every length up to 4096 is covered (radix kernels or chirp-z); longer lines with a
-    # large prime factor are not
+    # every length up to 4096 runs one pass kernel (radix or chirp-z) and longer lines a
+    # long-line step (four-step, or chirp-z for a large prime factor: 17 * 257 here); lines
+    # past 2^24 points are reported as unsupported
+    torch = torch_cuda
+    n = 17 * 257
+    x = np.random.default_rng(9).standard_normal(n) + 1j * np.random.default_rng(10).standard_normal(n)
+    xd = torch.tensor(x, dtype=torch.complex64, device="cuda")
+    X = torch.empty_like(xd)
+    F.Plan(F.C2CF, [n], dtype="float32").exec(xd, X)
+    torch.cuda.synchronize()
+    assert O.rel_l2(X.cpu().numpy(), np.fft.fft(x)) <= 5e-6
     with pytest.raises(F.FftbError) as e:
-        F.Plan(F.C2CF, [17 * 257], dtype="float32")
+        F.Plan(F.C2CF, [(1 << 24) + 2], dtype="float32")
     assert e.value.status == -2
 
 

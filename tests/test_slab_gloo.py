@@ -1,9 +1,10 @@
 """Host logic of the x-slab distributed 3D and 4D transforms (fftm_b200.slab) with
-world-size-2 `gloo` process groups on CPU: the slab decomposition, the all-to-all
-exchange and its packing, checked against numpy's full 3D / 4D transform (4D in both
-the slab [kx][ky][kz][kw] and fftm's native [ky][kz][kw][kx] spectrum orders).  The rank-local transforms are
-numpy stand-ins here (the library's GPU plans replace them on GPUs; one GPU per test
-box means the NCCL exchange itself is not run)."""
+world-size-2 `gloo` process groups on CPU: the slab decomposition and the all-to-all
+exchange of the send blocks, checked against numpy's full 3D / 4D transform (4D in both the
+slab [kx][ky][kz][kw] and fftm's native [ky][kz][kw][kx] spectrum orders).  The rank-local
+passes are the numpy stand-in of fftm_b200.slab (the same send / receive block semantics as
+the library's GPU passes, which replace it on GPUs; one GPU per test box means the NCCL
+exchange itself is not run)."""
 import json
 import os
 import socket
@@ -20,35 +21,15 @@ def _free_port():
     return port
 
 
-class _NumpyLocal:
-    def __init__(self, ny, nz, nx):
-        self.ny, self.nz, self.nx = ny, nz, nx
-
-    def r2c_yz(self, x, out):
-        import torch
-        out.copy_(torch.from_numpy(np.fft.rfftn(x.numpy(), axes=(1, 2))))
-
-    def c2r_yz(self, spec, out):
-        import torch
-        r = np.fft.irfftn(spec.numpy(), s=(self.ny, self.nz), axes=(1, 2)) * (self.ny * self.nz)
-        out.copy_(torch.from_numpy(r))
-
-    def fft_x(self, t, inverse=False):
-        import torch
-        a = t.numpy()
-        r = np.fft.ifft(a, axis=0) * self.nx if inverse else np.fft.fft(a, axis=0)
-        t.copy_(torch.from_numpy(r))
-
-
 def _rank_main(rank, world, port, outdir, dims):
     os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
     import torch
     import torch.distributed as dist
-    from fftm_b200.slab import SlabFFT3D
+    from fftm_b200.slab import SlabFFT3D, numpy_local
     dist.init_process_group("gloo", rank=rank, world_size=world)
     nx, ny, nz = dims
     g = np.random.default_rng(7).standard_normal(dims)
-    f = SlabFFT3D(nx, ny, nz, local=_NumpyLocal(ny, nz, nx))
+    f = SlabFFT3D(nx, ny, nz, local=numpy_local(dims, world))
     assert f.real_slab_shape() == (nx // world, ny, nz)
     xs = torch.from_numpy(np.ascontiguousarray(g[rank * f.nxl:(rank + 1) * f.nxl])).double()
     spec = f.forward(xs)
@@ -75,41 +56,25 @@ def test_slab_fft_two_ranks(tmp_path, dims):
 
 
 def test_slab_rejects_indivisible():
-    from fftm_b200.slab import SlabFFT3D
-    f = SlabFFT3D(6, 4, 8, local=_NumpyLocal(4, 8, 6))      # no process group: one rank
+    from fftm_b200.slab import SlabFFT3D, numpy_local
+    f = SlabFFT3D(6, 4, 8, local=numpy_local((6, 4, 8), 1))      # no process group: one rank
     assert f.P == 1 and f.spectrum_slab_shape() == (6, 4, 5)
-
-
-class _NumpyLocal4D:
-    def __init__(self, nz, nw, nx, ny, layout):
-        self.nz, self.nw, self.nx, self.ny, self.layout = nz, nw, nx, ny, layout
-
-    def r2c_zw(self, x, out):
-        import torch
-        out.copy_(torch.from_numpy(np.fft.rfftn(x.numpy(), axes=(2, 3))))
-
-    def c2r_zw(self, spec, out):
-        import torch
-        r = np.fft.irfftn(spec.numpy(), s=(self.nz, self.nw), axes=(2, 3)) * (self.nz * self.nw)
-        out.copy_(torch.from_numpy(r))
-
-    def fft_xy(self, t, inverse=False):
-        import torch
-        axes = (0, 3) if self.layout == "native_xzwy" else (0, 1)
-        a = t.numpy()
-        r = np.fft.ifftn(a, axes=axes) * (self.nx * self.ny) if inverse else np.fft.fftn(a, axes=axes)
-        t.copy_(torch.from_numpy(r))
+    # one rank: the exchange is nothing, and the host logic still transforms
+    import torch
+    g = np.random.default_rng(3).standard_normal((6, 4, 8))
+    spec = f.forward(torch.from_numpy(g))
+    assert np.linalg.norm(spec.numpy() - np.fft.rfftn(g)) / np.linalg.norm(np.fft.rfftn(g)) < 1e-12
 
 
 def _rank_main_4d(rank, world, port, outdir, dims, layout):
     os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
     import torch
     import torch.distributed as dist
-    from fftm_b200.slab import SlabFFT4D
+    from fftm_b200.slab import SlabFFT4D, numpy_local
     dist.init_process_group("gloo", rank=rank, world_size=world)
     nx, ny, nz, nw = dims
     g = np.random.default_rng(11).standard_normal(dims)
-    f = SlabFFT4D(nx, ny, nz, nw, layout=layout, local=_NumpyLocal4D(nz, nw, nx, ny, layout))
+    f = SlabFFT4D(nx, ny, nz, nw, layout=layout, local=numpy_local(dims, world, layout))
     assert f.real_slab_shape() == (nx // world, ny, nz, nw)
     xs = torch.from_numpy(np.ascontiguousarray(g[rank * f.nxl:(rank + 1) * f.nxl])).double()
     spec = f.forward(xs)
@@ -140,8 +105,8 @@ def test_slab_fft_4d_two_ranks(tmp_path, dims, layout):
 
 
 def test_slab_4d_rejects_indivisible_and_bad_layout():
-    from fftm_b200.slab import SlabFFT4D
-    f = SlabFFT4D(6, 4, 5, 8, local=_NumpyLocal4D(5, 8, 6, 4, "native_xzwy"))   # one rank
+    from fftm_b200.slab import SlabFFT4D, numpy_local
+    f = SlabFFT4D(6, 4, 5, 8, local=numpy_local((6, 4, 5, 8), 1, "native_xzwy"))   # one rank
     assert f.P == 1 and f.spectrum_slab_shape() == (4, 5, 5, 6)
     with pytest.raises(ValueError):
         SlabFFT4D(6, 4, 5, 8, layout="pencil", local=object())
