@@ -45,6 +45,19 @@ namespace fftb {
 __device__ __forceinline__ void cluster_arrive_relaxed() { asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory"); }
 __device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory"); }
 
+constexpr int kRingWaitLimit = 1 << 22;  // polls of a bounded bulk-copy wait (seconds)
+__device__ int g_ring_wait_error;        // set when a bounded wait gave up (a copy never completed)
+
+// 1D bulk copy global -> this CTA's shared memory (16-byte aligned addresses, size a
+// multiple of 16), completing on `bar`
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
 // ------------------------------------------------------------------ plane kernels
 // Work split (CL CTAs per plane, CL in {1, 2, 4, 8}):
 //   rows   : CTA c owns rows [c*M, (c+1)*M) for the z stage            (M = NY / CL)
@@ -287,6 +300,69 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
     const C *iplane = in + (size_t)x * NY * (NZ / 2 + 1);
     if constexpr (CL > 1) cluster_wait();  // every peer's shared memory exists from here on
 
+    // ---- stage y, one CTA per plane: the plane's spectrum rows [NY][NZ/2+1] are contiguous in
+    // global memory with the pitch of rowsm, so one bulk copy brings the whole plane in (no
+    // per-element transposing copies); each group reads its column into registers, and the
+    // inverse y FFT results go back to the same places (a spectrum that is not 16-byte
+    // aligned takes the staged path below)
+    bool bulk = false;
+    if constexpr (CL == 1) bulk = (reinterpret_cast<uintptr_t>(in) & 15) == 0;
+    if (bulk) {
+      if constexpr (CL == 1) {
+        constexpr int TY = S::TY, FY = S::FY;
+        constexpr unsigned BYTES = NY * (NZ / 2 + 1) * sizeof(C);
+        constexpr unsigned CHUNK = 16384;
+        static_assert(BYTES % 16 == 0 && S::PR == NZ / 2 + 1 && S::M == NY, "one plane per CTA");
+        __shared__ __align__(8) unsigned long long bar;
+        __shared__ int ok_s;
+        const int f = tid / TY, t = tid - (tid / TY) * TY;
+        if (tid == 0) {
+            mbar_init(&bar, 1);
+            mbar_init_fence();
+            mbar_arrive_expect_tx(&bar, BYTES);
+            for (unsigned o = 0; o < BYTES; o += CHUNK)
+                bulk_load(reinterpret_cast<char *>(rowsm) + o, reinterpret_cast<const char *>(iplane) + o,
+                          BYTES - o < CHUNK ? BYTES - o : CHUNK, &bar);
+        }
+        C twy[16];
+        load_stage_twiddles<R, NY>(twy, roots, S::NMAX, t);
+        C *reg = stg + f * RegFFTShape<NY>::REGION;
+        if (tid == 0) ok_s = mbar_wait(&bar, 0, kRingWaitLimit) ? 1 : 0;
+        __syncthreads();
+        if (!ok_s) {  // the copy never completed: flag it and leave
+            if (tid == 0) atomicExch(&g_ring_wait_error, 3);
+            return;
+        }
+#pragma unroll 1
+        for (int s0 = 0; s0 < S::S; s0 += FY) {
+            const int sl = s0 + f;
+            const bool ok = sl < S::S;
+            const int slc = ok ? sl : 0;
+            C v[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) v[r] = rowsm[(t + TY * r) * S::PR + slc];
+            if (ok && sl == 0) {
+                // the packed slot (see the cluster path below), partners read from the plane
+#pragma unroll
+                for (int r = 0; r < 16; ++r) {
+                    const int ky = t + TY * r, km = (NY - ky) & (NY - 1);
+                    const C x0m = rowsm[km * S::PR];
+                    const C xnk = rowsm[ky * S::PR + S::NS];
+                    const C xnm = rowsm[km * S::PR + S::NS];
+                    const C h0 = cscale(cadd(v[r], cconj(x0m)), R(0.5));
+                    const C hn = cscale(cadd(xnk, cconj(xnm)), R(0.5));
+                    v[r] = mk<R>(h0.x - hn.y, h0.y + hn.x);
+                }
+            }
+            __syncthreads();  // this block's columns (and the packed partners) are read
+            regfft_warp_rt<R, NY, +1>(v, reg, twy, t);
+            if (ok) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) rowsm[(t + TY * j) * S::PR + sl] = v[j];
+            }
+        }
+      }
+    } else {
     // ---- stage y: inverse FFT of the owned slots, rows pushed to their owners
     {
         constexpr int TY = S::TY, FY = S::FY;
@@ -361,6 +437,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
             __syncthreads();  // the staging area is refilled for the next block
             if (s0 + FY < S::S) stage(s0 + FY, stg);
         }
+    }
     }
     if constexpr (CL > 1) cg::this_cluster().sync();
     else __syncthreads();
@@ -632,8 +709,6 @@ __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data,
 // FFTs, so the ring is the only shared memory the kernel needs; each thread keeps its
 // stage twiddles w_NX^(t k1) in registers for every tile it transforms.
 constexpr int kRingStages = 3;
-constexpr int kRingWaitLimit = 1 << 22;  // polls of a bounded bulk-copy wait (seconds)
-__device__ int g_ring_wait_error;        // set when a bounded wait gave up (a copy never completed)
 
 template <typename R, int NX>
 __device__ __forceinline__ void xcol_fft_regtw(cpx<R> (&v)[16], cpx<R> *scr, const cpx<R> (&tw)[16], int t, int col,
