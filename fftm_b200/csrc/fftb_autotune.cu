@@ -548,6 +548,16 @@ int measure_ffts(int dtype, long long nx, long long ny, long long nz, long long 
     if (dim == 3) {
         int cl[4];
         const int n = fused3d_clusters(dtype, nx, ny, nz, cl, 4);
+        if (n > 0) {
+            // the library's own choice: the smallest cluster that fits for the forward planes,
+            // and for the inverse planes a larger one when that doubles their CTAs per SM
+            // (a pair no forced cluster size gives)
+            Candidate c;
+            c.name = "fused";
+            c.a = FFTB_STRATEGY_FUSED;
+            c.b = 0;
+            cands.push_back(c);
+        }
         for (int i = 0; i < n; ++i) {
             Candidate c;
             c.name = "fused-cl" + std::to_string(cl[i]);

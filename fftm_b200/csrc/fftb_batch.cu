@@ -62,9 +62,11 @@ __device__ __forceinline__ int ld_acquire(const int *p)
 // register allocation instead of the union of all of them.  The tile stages its lines
 // with cp.async: thread 0's acquire load of the producer counters followed by the
 // CTA barrier orders these loads after the producers' fenced stores (PTX memory model).
-template <int NF> __device__ __noinline__ void batch_tile(const PassArgs *a, long long line0, unsigned char *smem)
+template <int NF>
+__device__ __noinline__ void batch_tile(const PassArgs *a, const void *in, void *out, long long line0,
+                                        unsigned char *smem)
 {
-    pass_body<float, NF, false>(*a, line0, smem);
+    pass_body<float, NF, false, false>(*a, in, out, line0, smem);
 }
 
 // ctl[0]: queue head, ctl[1]: error flag, ctl[2 + p]: finished tiles of pass p
@@ -105,16 +107,16 @@ __global__ void __launch_bounds__(kBatchThreads)
         __syncthreads();
         if (it >= nitems || !ok) break;
         const BatchItem bi = items[it];
-        PassArgs a = passes[bi.pass];
+        const PassArgs *a = passes + bi.pass;
         const PassBind b = binds[bi.pass];
         const void *bufs[3] = {in, out, work};
-        a.in = (const char *)bufs[b.in_buf] + b.in_off;
-        a.out = (char *)bufs[b.out_buf] + b.out_off;
-        const long long line0 = (long long)bi.tile * a.G;
+        const void *pin = (const char *)bufs[b.in_buf] + b.in_off;
+        void *pout = (char *)const_cast<void *>(bufs[b.out_buf]) + b.out_off;
+        const long long line0 = (long long)bi.tile * a->G;
         switch (b.nf) {
 #define FFTB_CASE(n)                                                                                                  \
     case n:                                                                                                           \
-        batch_tile<n>(&a, line0, smem_raw);                                                                           \
+        batch_tile<n>(a, pin, pout, line0, smem_raw);                                                                 \
         break;
             FFTB_BATCH_NF_LIST(FFTB_CASE)
 #undef FFTB_CASE
@@ -145,11 +147,11 @@ __global__ void __launch_bounds__(kBatchThreads)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const BatchItem bi = items[blockIdx.x];
-    PassArgs a = passes[bi.pass];
+    const PassArgs &a = passes[bi.pass];
     const PassBind b = binds[bi.pass];
-    a.in = (const char *)batch_buf(b.in_buf, in, out, work) + b.in_off;
-    a.out = (char *)const_cast<void *>(batch_buf(b.out_buf, in, out, work)) + b.out_off;
-    pass_body<float, NF, false>(a, (long long)bi.tile * a.G, smem_raw);
+    const void *pin = (const char *)batch_buf(b.in_buf, in, out, work) + b.in_off;
+    void *pout = (char *)const_cast<void *>(batch_buf(b.out_buf, in, out, work)) + b.out_off;
+    pass_body<float, NF, false, false>(a, pin, pout, (long long)bi.tile * a.G, smem_raw);
 }
 
 const void *batch_group_fn(int nf)

@@ -95,9 +95,15 @@ template <typename R> __device__ __forceinline__ R ep_factor(const PassArgs &a, 
 }
 
 // One CTA's share of a pass: the G lines starting at line0.  Any block size works;
-// threads past G * threads_per_line(NF) only join the barriers.
-template <typename R, int NF, bool CG>
-__device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, unsigned char *smem_raw)
+// threads past G * threads_per_line(NF) only join the barriers.  EXT compiles in the
+// blocked point indices (slab exchanges) and the four-step twiddle epilogue (long lines);
+// callers that never use them (the batch kernels) leave them out, which keeps their
+// register count and occupancy.
+// The line buffers are in_ptr / out_ptr (a.in / a.out for a plain launch; the batch kernels
+// bind theirs per item without copying the argument struct).
+template <typename R, int NF, bool CG, bool EXT = true>
+__device__ __forceinline__ void pass_body(const PassArgs &a, const void *in_ptr, void *out_ptr, long long line0,
+                                          unsigned char *smem_raw)
 {
     using C = cpx<R>;
     constexpr int T = threads_per_line(NF);
@@ -143,23 +149,38 @@ __device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, un
     const long long is = a.is, os = a.os;
 
     // ------------------------------------------------------------ load (asynchronous copies)
-    const void *gdummy = a.in;
+    const void *gdummy = in_ptr;
     if (kind == K_C2C_FWD || kind == K_C2C_INV || kind == K_SANDWICH) {
-        const C *in = reinterpret_cast<const C *>(a.in);
+        const C *in = reinterpret_cast<const C *>(in_ptr);
         const int tot = G * NF;
+        // the blocked point index (a slab exchange's unpack) gets a loop of its own, so the
+        // plain loop carries none of its index arithmetic
+        if (EXT && a.in_blk) {
+            const int blk = a.in_blk;
+            const long long hi = a.in_hi;
+            for (int e = tid; e < tot; e += blockDim.x) {
+                int gg, p;
+                if (a.in_pts_fast) { gg = e / NF; p = e - gg * NF; }
+                else { gg = e & (G - 1); p = e >> gshift; }
+                const bool ok = bidx[4 * gg + 3] != 0;
+                const int q = p / blk;
+                const long long pi = (long long)q * hi + (long long)(p - q * blk) * is;
+                stage_load<CG, sizeof(C)>(&lines[gg * LP + pad16(p)],
+                                          ok ? (const void *)(in + offs[2 * gg] + pi) : gdummy, ok);
+            }
+        } else {
 #pragma unroll 4
-        for (int e = tid; e < tot; e += blockDim.x) {
-            int gg, p;
-            if (a.in_pts_fast) { gg = e / NF; p = e - gg * NF; }
-            else { gg = e & (G - 1); p = e >> gshift; }
-            const bool ok = bidx[4 * gg + 3] != 0;
-            const long long pi = a.in_blk ? (long long)(p / a.in_blk) * a.in_hi + (long long)(p % a.in_blk) * is
-                                          : (long long)p * is;
-            stage_load<CG, sizeof(C)>(&lines[gg * LP + pad16(p)], ok ? (const void *)(in + offs[2 * gg] + pi) : gdummy,
-                                ok);
+            for (int e = tid; e < tot; e += blockDim.x) {
+                int gg, p;
+                if (a.in_pts_fast) { gg = e / NF; p = e - gg * NF; }
+                else { gg = e & (G - 1); p = e >> gshift; }
+                const bool ok = bidx[4 * gg + 3] != 0;
+                stage_load<CG, sizeof(C)>(&lines[gg * LP + pad16(p)],
+                                          ok ? (const void *)(in + offs[2 * gg] + p * is) : gdummy, ok);
+            }
         }
     } else if (kind == K_R2C) {
-        const R *in = reinterpret_cast<const R *>(a.in);
+        const R *in = reinterpret_cast<const R *>(in_ptr);
         const int tot = G * NF;
 #pragma unroll 4
         for (int e = tid; e < tot; e += blockDim.x) {
@@ -182,7 +203,7 @@ __device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, un
             }
         }
     } else { // K_C2R
-        const C *in = reinterpret_cast<const C *>(a.in);
+        const C *in = reinterpret_cast<const C *>(in_ptr);
         const int nin = a.half ? NF + 1 : NF / 2 + 1;
         const int tot = G * nin;
 #pragma unroll 4
@@ -265,7 +286,7 @@ __device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, un
     // ------------------------------------------------------------ store
     const bool ep_store = (a.ep_mode != 0) && kind != K_SANDWICH;
     if (kind == K_C2R) {
-        R *out = reinterpret_cast<R *>(a.out);
+        R *out = reinterpret_cast<R *>(out_ptr);
         const R sc = R(a.ep_scale);
         if (a.half) {
             const int tot = G * NF;
@@ -293,30 +314,51 @@ __device__ __forceinline__ void pass_body(const PassArgs &a, long long line0, un
             }
         }
     } else {
-        C *out = reinterpret_cast<C *>(a.out);
+        C *out = reinterpret_cast<C *>(out_ptr);
         const int nout = (kind == K_R2C) ? (a.half ? NF + 1 : NF / 2 + 1) : NF;
         const int tot = G * nout;
-        const bool twid = (a.ep_mode & EP_TWIDDLE) != 0;
-        const bool fct = ep_store && (a.ep_mode & ~EP_TWIDDLE) != 0;
-        const C *eptw = reinterpret_cast<const C *>(a.ep_tw);
-#pragma unroll 4
-        for (int e = tid; e < tot; e += blockDim.x) {
-            int gg, p;
-            if (a.out_pts_fast) { gg = e / nout; p = e - gg * nout; }
-            else { gg = e & (G - 1); p = e >> gshift; }
-            if (!bidx[4 * gg + 3]) continue;
-            C v = lines[gg * LP + pad16(p)];
-            if (twid) {
-                // p < L1 and j < L2, so p * j < L: no reduction needed
-                const C w = eptw[(long long)p * bidx[4 * gg + a.ep_src[0] - 1]];
-                v = kind == K_C2C_INV ? cmulc(v, w) : cmul(v, w);
+        if (EXT && ((a.ep_mode & EP_TWIDDLE) || a.out_blk)) {
+            // the four-step twiddle (long lines) and the blocked store (a slab exchange's
+            // pack, optionally into peer buffers) in a loop of their own
+            const bool twid = (a.ep_mode & EP_TWIDDLE) != 0;
+            const bool fct = ep_store && (a.ep_mode & ~EP_TWIDDLE) != 0;
+            const C *eptw = reinterpret_cast<const C *>(a.ep_tw);
+            for (int e = tid; e < tot; e += blockDim.x) {
+                int gg, p;
+                if (a.out_pts_fast) { gg = e / nout; p = e - gg * nout; }
+                else { gg = e & (G - 1); p = e >> gshift; }
+                if (!bidx[4 * gg + 3]) continue;
+                C v = lines[gg * LP + pad16(p)];
+                if (twid) {
+                    // p < L1 and j < L2, so p * j < L: no reduction needed
+                    const C w = eptw[(long long)p * bidx[4 * gg + a.ep_src[0] - 1]];
+                    v = kind == K_C2C_INV ? cmulc(v, w) : cmul(v, w);
+                }
+                if (fct) v = cscale(v, ep_factor<R>(a, p, bidx + 4 * gg));
+                if (a.out_blk) {
+                    const int q = p / a.out_blk;
+                    // select the peer pointer with compile-time indices: a dynamic index into
+                    // the argument struct would move the whole struct to local memory in the
+                    // kernels that copy it
+                    void *peer = nullptr;
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        if (i == q) peer = a.out_peer[i];
+                    C *base = peer ? reinterpret_cast<C *>(peer) : out + (long long)q * a.out_hi;
+                    base[offs[2 * gg + 1] + (long long)(p - q * a.out_blk) * os] = v;
+                } else {
+                    out[offs[2 * gg + 1] + p * os] = v;
+                }
             }
-            if (fct) v = cscale(v, ep_factor<R>(a, p, bidx + 4 * gg));
-            if (a.out_blk) {
-                const int q = p / a.out_blk;
-                C *base = a.out_peer[q] ? reinterpret_cast<C *>(a.out_peer[q]) : out + (long long)q * a.out_hi;
-                base[offs[2 * gg + 1] + (long long)(p - q * a.out_blk) * os] = v;
-            } else {
+        } else {
+#pragma unroll 4
+            for (int e = tid; e < tot; e += blockDim.x) {
+                int gg, p;
+                if (a.out_pts_fast) { gg = e / nout; p = e - gg * nout; }
+                else { gg = e & (G - 1); p = e >> gshift; }
+                if (!bidx[4 * gg + 3]) continue;
+                C v = lines[gg * LP + pad16(p)];
+                if (ep_store) v = cscale(v, ep_factor<R>(a, p, bidx + 4 * gg));
                 out[offs[2 * gg + 1] + p * os] = v;
             }
         }
@@ -327,7 +369,7 @@ template <typename R, int NF>
 __global__ void __launch_bounds__(512) fftb_pass_kernel(PassArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    pass_body<R, NF, false>(a, (long long)blockIdx.x * a.G, smem_raw);
+    pass_body<R, NF, false>(a, a.in, a.out, (long long)blockIdx.x * a.G, smem_raw);
 }
 
 template <typename R, int NF> inline PassKernelInfo pass_kernel_info()
