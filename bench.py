@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="fftb", choices=["fftb", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--strategy", choices=["fused", "staged", "fused_tc"],
+                    help="run the headline solve with this strategy instead of the autotuner's choice")
     # profiling mode: run one workload a fixed number of times and nothing else, so that a
     # profiler (ncu -k ... -s ... -c ...) sees a short, predictable launch sequence
     ap.add_argument("--profile-case", choices=["poisson3d", "staged3d", "roundtrip4d", "batch"])
@@ -349,8 +351,14 @@ def main():
     # execution strategy from the project autotuner (fresh cache per run: a measured sweep of
     # the fused plane-cluster sizes and the staged passes, least median of forward+backward)
     import tempfile
-    with tempfile.TemporaryDirectory() as td:
-        tuned = ff.autotune(os.path.join(td, "fftm_autotune_3d.env"))
+    if args.strategy:
+        # a fixed strategy instead of the measured one (for ncu launch lists: under ncu the
+        # profiled kernels run slower, which would bias the autotuner's choice)
+        ff.set_strategy(args.strategy)
+        tuned = None
+    else:
+        with tempfile.TemporaryDirectory() as td:
+            tuned = ff.autotune(os.path.join(td, "fftm_autotune_3d.env"))
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.float32, device=dev)   # 1 GiB > L2
     stream = torch.cuda.current_stream()
 
@@ -407,16 +415,19 @@ def main():
 
     # end to end through the public API with host buffers (pinned), copies inside the timed region.
     # Every step copies its right-hand side host -> device, solves, and copies the solution
-    # device -> host.  Two buffer sets and two streams let step i+1's upload (one copy engine)
-    # run while step i solves and downloads (the other engine), as a serving loop would; the
-    # same loop with one stream (each copy after the previous step) is reported beside it.
+    # device -> host.  Two buffer sets and three streams (upload, solve, download) let step
+    # i+1's upload (one copy engine) and step i-1's download (the other engine) run while step
+    # i solves, as a serving loop would, so the step time approaches one PCIe transfer of the
+    # field; the same loop with one stream (each copy after the previous step) is reported
+    # beside it.
     h_in = torch.from_numpy(f_host).pin_memory()
     h_out = [torch.empty_like(h_in).pin_memory() for _ in range(2)]
     d_in = [torch.empty_like(rhs) for _ in range(2)]
     d_out = [torch.empty_like(rhs) for _ in range(2)]
-    s_in, s_cmp = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
-    ev_in = [torch.cuda.Event() for _ in range(2)]
-    ev_done = [torch.cuda.Event() for _ in range(2)]
+    s_in, s_cmp, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    ev_in = [torch.cuda.Event() for _ in range(2)]        # upload of buffer set b done
+    ev_solved = [torch.cuda.Event() for _ in range(2)]    # solve of set b done (d_in[b] free)
+    ev_out = [torch.cuda.Event() for _ in range(2)]       # download of set b done (d_out[b] free)
     e2e_steps = max(3, min(args.steps, 20))
 
     def e2e_pipelined(nsteps):
@@ -424,14 +435,19 @@ def main():
             b = i % 2
             with torch.cuda.stream(s_in):
                 if i >= 2:
-                    s_in.wait_event(ev_done[b])
+                    s_in.wait_event(ev_solved[b])
                 d_in[b].copy_(h_in, non_blocking=True)
                 ev_in[b].record(s_in)
             with torch.cuda.stream(s_cmp):
                 s_cmp.wait_event(ev_in[b])
+                if i >= 2:
+                    s_cmp.wait_event(ev_out[b])
                 ff.poisson(d_in[b], d_out[b], -1.0, stream=s_cmp)
+                ev_solved[b].record(s_cmp)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_solved[b])
                 h_out[b].copy_(d_out[b], non_blocking=True)
-                ev_done[b].record(s_cmp)
+                ev_out[b].record(s_out)
 
     def e2e_serial(nsteps):
         for _ in range(nsteps):
@@ -446,8 +462,9 @@ def main():
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(s_in)
     s_cmp.wait_event(e0)
+    s_out.wait_event(e0)
     e2e_pipelined(e2e_steps)
-    e1.record(s_cmp)
+    e1.record(s_out)   # after the last download, which follows every earlier copy and solve
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
     e2e_ms = replicas.max_over_ranks(dist, e2e_ms, dev)
@@ -833,8 +850,8 @@ def main():
         "gflops": FLOPS_RT / (total_ms / args.steps * 1e-3) / 1e9,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": DATA,
         "config": {"workload": WORKLOAD, "n": [NX, NY, NZ], "bytes_per_step": BYTES_RT,
-                   "strategy": tuned.config.get("FFTM_AUTOTUNE_STRATEGY_3D"),
-                   "autotune_median_ms": tuned.medians_ms(),
+                   "strategy": tuned.config.get("FFTM_AUTOTUNE_STRATEGY_3D") if tuned else args.strategy,
+                   "autotune_median_ms": tuned.medians_ms() if tuned else None,
                    "l2": "flushed between steps (1 GiB write outside the timed window)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "gpu_launches": launches_per_step * args.steps,
@@ -844,7 +861,7 @@ def main():
         "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": int(rhs.numel() * 4),
                 "d2h_bytes_per_step": int(sol.numel() * 4), "steps": e2e_steps,
                 "ms_per_step": e2e_ms / e2e_steps,
-                "pipelining": "two buffer sets, upload of step i+1 overlaps solve + download of step i",
+                "pipelining": "two buffer sets, three streams: upload of step i+1 and download of step i-1 overlap the solve of step i",
                 "serial_ms_per_step": e2e_serial_ms / e2e_steps,
                 "serial_value": BYTES_RT * e2e_steps / (e2e_serial_ms * 1e-3) / 1e9,
                 "solutions_identical": e2e_ok},

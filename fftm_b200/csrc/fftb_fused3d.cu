@@ -333,9 +333,16 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
             if (tid == 0) atomicExch(&g_ring_wait_error, 3);
             return;
         }
+        // slot of this group within a block of FY slots: the G = 32 / TY groups of a warp take
+        // slots TY apart, so the warp's 32 column reads (rows t + TY r, row pitch NZ/2 + 1,
+        // one mod 16 in 8-byte words) cover the 16 bank pairs twice each, the minimum for 256
+        // bytes; consecutive slots would hit 11 bank pairs, up to 4 lanes each
+        constexpr int G = 32 / TY, W = S::NT / 32;
+        const int g = f % G, w = f / G;
+        const int perm = W >= TY ? g * TY + w % TY + (w / TY) * 32 : w + W * g;
 #pragma unroll 1
         for (int s0 = 0; s0 < S::S; s0 += FY) {
-            const int sl = s0 + f;
+            const int sl = s0 + perm;
             const bool ok = sl < S::S;
             const int slc = ok ? sl : 0;
             C v[16];
