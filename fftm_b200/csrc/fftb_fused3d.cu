@@ -131,6 +131,14 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *plane = reinterpret_cast<C *>(smem_raw);   // [NY][PF]: this CTA's column slots
     C *scr = plane + NY * S::PF;
+    // Row `row` starts at row * PF + skew(row).  With four threads per z FFT, the eight row
+    // pairs a warp pushes at once sit 2 PF apart, which is 8 words mod 16 when PF = 4 mod 16
+    // (what the y stage's column reads need), so they would share half the bank pairs; the
+    // skew (4 entries on every other row pair, inside the row padding) spreads them over all
+    // 16.  It is constant across the rows t + TY r one column read touches, so the column
+    // reads keep their spread.
+    constexpr int SKEW = (S::TZ == 4 && (2 * S::PF) % 16 == 8 && S::PF - S::S >= 4) ? 4 : 0;
+    auto row_at = [&](int row) { return row * S::PF + SKEW * ((row >> 2) & 1); };
     if constexpr (CL > 1) cluster_arrive_relaxed();
     const int tid = threadIdx.x;
     const int c = (CL > 1) ? (int)cg::this_cluster().block_rank() : 0;
@@ -211,8 +219,8 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
                 if (ok) {
                     const int owner = k / S::S, ls = k - owner * S::S;
                     C *d = dst[owner];
-                    d[ya * S::PF + ls] = A;
-                    d[(ya + 1) * S::PF + ls] = B;
+                    d[row_at(ya) + ls] = A;
+                    d[row_at(ya + 1) + ls] = B;
                 }
             }
             __syncwarp();
@@ -236,7 +244,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
             const int slc = ok ? sl : 0;
             C v[16];
 #pragma unroll
-            for (int r = 0; r < 16; ++r) v[r] = plane[(t + TY * r) * S::PF + slc];
+            for (int r = 0; r < 16; ++r) v[r] = plane[row_at(t + TY * r) + slc];
             regfft_warp_rt<R, NY, -1>(v, reg, twy, t);
             // the packed slot (slot 0 of CTA 0, first round, warp 0):
             // X0[ky] = (W[ky] + conj W[-ky]) / 2, XN[ky] = (W[ky] - conj W[-ky]) / 2i
@@ -259,7 +267,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
             }
             if (ok) {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) plane[(t + TY * j) * S::PF + slc] = v[j];
+                for (int j = 0; j < 16; ++j) plane[row_at(t + TY * j) + slc] = v[j];
             }
             // coalesced row-segment stores of this round's slots, out[x][ky][c*S + s]; they
             // drain while the next round computes
@@ -270,7 +278,7 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
 #pragma unroll 4
             for (int e = tid; e < NY * ns; e += S::NT) {
                 const int row = e / ns, q = e - (e / ns) * ns;
-                orow[(size_t)row * (NZ / 2 + 1) + q] = plane[row * S::PF + s0 + q];
+                orow[(size_t)row * (NZ / 2 + 1) + q] = plane[row_at(row) + s0 + q];
             }
         }
     }
