@@ -16,11 +16,14 @@
 
 namespace fftb {
 
-// Power-of-two lines of 32..256 points run the register-resident two-stage FFT
-// (fftb_regfft.cuh) on their staged line instead of the Stockham passes: one read of
-// the line into registers, radix-16 in registers, one exchange through the line's own
-// buffer, the second stage in registers, one write back.
-template <int NF> constexpr bool pass_regfft() { return NF >= 32 && NF <= 256 && (NF & (NF - 1)) == 0; }
+// Lines of 16 T points (T = 2..16 a power of two, or T = 3, 5, 6: 48, 80 and 96 points) run
+// the register-resident two-stage FFT (fftb_regfft.cuh) on their staged line instead of the
+// Stockham passes: one read of the line into registers, radix-16 in registers, one exchange
+// through the line's own buffer, T-point DFTs in registers, one write back.
+template <int NF> constexpr bool pass_regfft()
+{
+    return (NF >= 32 && NF <= 256 && (NF & (NF - 1)) == 0) || NF == 48 || NF == 80 || NF == 96;
+}
 
 // pitch of a staged line: the padded line, or the register FFT's exchange region if larger
 template <int NF> constexpr int pass_line_pitch()
@@ -34,7 +37,49 @@ template <int NF> constexpr int pass_line_pitch()
 template <typename R, int NF, int SIGN>
 __device__ __forceinline__ void line_fft(cpx<R> *ln, cpx<R> *lnp, const cpx<R> *tw, int ntw, int t, bool act)
 {
-    if constexpr (pass_regfft<NF>()) {
+    if constexpr (pass_regfft<NF>() && 16 % RegFFTShape<NF>::T != 0) {
+        // T = 3, 5, 6 threads per line: a line's threads may straddle two warps, so the
+        // exchange is ordered by block barriers; thread t runs the second-stage DFTs of
+        // k1 = t, t + T, ... < 16 and holds their results until every thread has read the
+        // exchange region, then writes X[k1 + 16 k2]
+        using C = cpx<R>;
+        using S = RegFFTShape<NF>;
+        constexpr int T = S::T;
+        constexpr int A = (16 + T - 1) / T;
+        const int rs = ntw / NF;
+        C v[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) v[r] = act ? ln[pad16(t + T * r)] : mk<R>(R(0), R(0));
+        __syncthreads();  // every line is read before the exchanges overwrite it
+        dft16<SIGN, C, R>(v);
+#pragma unroll
+        for (int k1 = 1; k1 < 16; ++k1) v[k1] = twiddle_mul<SIGN>(v[k1], tw, (t * k1) * rs);
+        if (act) {
+#pragma unroll
+            for (int k1 = 0; k1 < 16; ++k1) ln[k1 * S::ROWP + t] = v[k1];
+        }
+        __syncthreads();
+        C res[A][T];
+#pragma unroll
+        for (int a = 0; a < A; ++a) {
+            const int k1 = t + T * a;
+#pragma unroll
+            for (int q = 0; q < T; ++q) res[a][q] = (act && k1 < 16) ? ln[k1 * S::ROWP + q] : mk<R>(R(0), R(0));
+            dft_small<SIGN, T, C, R>(res[a]);
+        }
+        __syncthreads();  // the exchange regions are read before the results overwrite them
+        if (act) {
+#pragma unroll
+            for (int a = 0; a < A; ++a) {
+                const int k1 = t + T * a;
+                if (k1 < 16) {
+#pragma unroll
+                    for (int k2 = 0; k2 < T; ++k2) ln[pad16(k1 + 16 * k2)] = res[a][k2];
+                }
+            }
+        }
+        __syncthreads();
+    } else if constexpr (pass_regfft<NF>()) {
         using C = cpx<R>;
         using S = RegFFTShape<NF>;
         constexpr int T = S::T;

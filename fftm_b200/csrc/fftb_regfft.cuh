@@ -23,11 +23,36 @@ template <int N> struct RegFFTShape {
     static constexpr int REGION = (T == 1) ? 16 : 16 * ROWP + (T == 16 ? 0 : T);
 };
 
+// In-order DFT of 6 values: X[k] = E[k] + w6^k O[k], X[k + 3] = E[k] - w6^k O[k] with E, O the
+// 3-point DFTs of the even and odd samples (Cooley-Tukey, 6 = 2 x 3).
+template <int SIGN, typename C, typename R> __device__ __forceinline__ void dft6(C *u)
+{
+    C e[3] = {u[0], u[2], u[4]}, o[3] = {u[1], u[3], u[5]};
+    dft3<SIGN, C, R>(e);
+    dft3<SIGN, C, R>(o);
+    const R h = R(0.5), s3 = kconst<R>::s3;
+    // w6^1 = 1/2 + SIGN i s3, w6^2 = -1/2 + SIGN i s3
+    const C o1 = mk<R>(h * o[1].x - SIGN * s3 * o[1].y, h * o[1].y + SIGN * s3 * o[1].x);
+    const C o2 = mk<R>(-h * o[2].x - SIGN * s3 * o[2].y, -h * o[2].y + SIGN * s3 * o[2].x);
+    u[0] = cadd(e[0], o[0]);
+    u[3] = csub(e[0], o[0]);
+    u[1] = cadd(e[1], o1);
+    u[4] = csub(e[1], o1);
+    u[2] = cadd(e[2], o2);
+    u[5] = csub(e[2], o2);
+}
+
 template <int SIGN, int L, typename C, typename R> __device__ __forceinline__ void dft_small(C *u)
 {
     if constexpr (L == 1) {
     } else if constexpr (L == 2) {
         dft2<SIGN>(u[0], u[1]);
+    } else if constexpr (L == 3) {
+        dft3<SIGN, C, R>(u);
+    } else if constexpr (L == 5) {
+        dft5<SIGN, C, R>(u);
+    } else if constexpr (L == 6) {
+        dft6<SIGN, C, R>(u);
     } else if constexpr (L == 4) {
         dft4<SIGN>(u[0], u[1], u[2], u[3]);
     } else if constexpr (L == 8) {
