@@ -172,7 +172,8 @@ void plan_registry()
            "incompatible exec direction -> std::logic_error");
     int status = 0;
     try {
-        fftb::fft<float, fftb::direction::C2CF> big(std::array<long long, 1>{17 * 257}, 1);
+        // every length up to 2^24 points has a kernel (radix, chirp-z or the long-line step)
+        fftb::fft<float, fftb::direction::C2CF> big(std::array<long long, 1>{(1LL << 24) + 2}, 1);
     } catch (const fftb::error &e) {
         status = e.status();
     }
