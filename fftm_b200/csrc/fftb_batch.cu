@@ -29,6 +29,7 @@
 
 #include "../../include/fftb.h"
 #include "fftb_engine.h"
+#include "fftb_fused3d.h"
 #include "fftb_pass.cuh"
 
 namespace fftb {
@@ -220,9 +221,18 @@ struct OpPlan {
     struct Group {
         int offset, count, nf;
         size_t smem;
+        // x and y stages of lengths with a column kernel: one grouped column-kernel launch
+        // over count tiles (XGroupItem offset ..) instead of the pass items
+        bool xcol = false;
+        int ckind = 0;        // col_group kind: 0/1/2 x forward / inverse / sandwich, 3/4 y
+        int buf = B_WORK;     // the buffer holding the spectra (in place)
+        void *roots = nullptr;
+        int ep_mode = 0;      // the sandwich's multiply (the pass epilogue)
+        double ep_scale = 1.0, ep_sign = -1.0;
     };
     std::vector<Group> groups;
     BatchItem *d_gitems = nullptr;
+    XGroupItem *d_xitems = nullptr;
     // CUDA graph of the persistent launch (mode 2) or of the grouped launches (mode 4)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -368,15 +378,55 @@ int build_plan(fftb_batch_s *b, int op, double sign)
         }
     P.nitems = (int)items.size();
     P.smem = smem;
-    // grouped order: within each stage, the items of each line length together
+    // grouped order: within each stage, the items of each line length together; the x and y
+    // stages of lengths that have a column kernel run as one grouped column-kernel launch
+    // each (the fused 3D path's register-resident column FFT, tiles of W lines)
     std::vector<BatchItem> gitems;
+    std::vector<XGroupItem> xitems;
     gitems.reserve(items.size());
     for (int s = 0; s < P.nstages; ++s) {
         std::vector<int> nfs;
         for (int i = 0; i < b->count; ++i) nfs.push_back(binds[tpass[i][s]].nf);
         std::sort(nfs.begin(), nfs.end());
         nfs.erase(std::unique(nfs.begin(), nfs.end()), nfs.end());
+        // the stage's column kind: x passes step C3 = ny * nzh between points, y passes nzh
+        int ckind = -1;
+        {
+            const Launch &L0 = P.seq.launches[tpass[0][s]];
+            const PassArgs &a0 = L0.args;
+            const long long ny0 = b->dims[1], nzh0 = b->dims[2] / 2 + 1;
+            const bool inplace = L0.in_buf == L0.out_buf && L0.in_off_bytes == L0.out_off_bytes;
+            if (b->dtype == FFTB_F32 && inplace && L0.longline == nullptr && a0.bs_n == 0 && ny0 > 1) {
+                if (a0.kind == K_SANDWICH && a0.is == ny0 * nzh0) ckind = 2;
+                else if ((a0.kind == K_C2C_FWD || a0.kind == K_C2C_INV) && a0.ep_mode == 0)
+                    ckind = a0.is == ny0 * nzh0 ? (a0.kind == K_C2C_FWD ? 0 : 1)
+                                                : (a0.is == nzh0 ? (a0.kind == K_C2C_FWD ? 3 : 4) : -1);
+            }
+        }
         for (int nf : nfs) {
+            const int W = ckind >= 0 ? col_group_tile_lines(b->dtype, nf) : 0;
+            if (W > 0) {
+                OpPlan::Group g{(int)xitems.size(), 0, nf, 0, true, ckind, B_WORK, nullptr};
+                const Launch &L0 = P.seq.launches[tpass[0][s]];
+                g.buf = L0.in_buf;
+                g.ep_mode = L0.args.ep_mode;
+                g.ep_scale = L0.args.ep_scale;
+                g.ep_sign = L0.args.ep_sign;
+                int st = col_group_prepare(b->dtype, ckind, nf, &g.roots);
+                if (st != FFTB_SUCCESS) return st;
+                for (int i = 0; i < b->count; ++i) {
+                    const long long nx = b->dims[3 * i], ny = b->dims[3 * i + 1], nz = b->dims[3 * i + 2];
+                    if ((ckind <= 2 ? nx : ny) != nf) continue;
+                    const Launch &L = P.seq.launches[tpass[i][s]];
+                    const long long lines = (ckind <= 2 ? ny : nx) * (nz / 2 + 1);
+                    for (long long t = 0; t < (lines + W - 1) / W; ++t)
+                        xitems.push_back(XGroupItem{(long long)(L.in_off_bytes / complex_bytes(b->dtype)),
+                                                    (int)lines, (int)t, (int)ny, (int)nz});
+                }
+                g.count = (int)xitems.size() - g.offset;
+                if (g.count > 0) P.groups.push_back(g);
+                continue;
+            }
             OpPlan::Group g{(int)gitems.size(), 0, nf, 0};
             for (int i = 0; i < b->count; ++i) {
                 const int p = tpass[i][s];
@@ -394,7 +444,8 @@ int build_plan(fftb_batch_s *b, int op, double sign)
                      s_binds = al(binds.size() * sizeof(PassBind)), s_deps = al(deps.size() * sizeof(int)),
                      s_nt = al(ntiles.size() * sizeof(int)), s_ctl = al((2 + P.npasses) * sizeof(int));
         const size_t s_gitems = al(gitems.size() * sizeof(BatchItem));
-        const size_t tot = s_items + s_args + s_binds + s_deps + s_nt + s_ctl + s_gitems;
+        const size_t s_xitems = al(xitems.size() * sizeof(XGroupItem));
+        const size_t tot = s_items + s_args + s_binds + s_deps + s_nt + s_ctl + s_gitems + s_xitems;
         cudaError_t e = cudaMalloc(&P.blob, tot);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -407,7 +458,8 @@ int build_plan(fftb_batch_s *b, int op, double sign)
         P.d_deps = (int *)q; q += s_deps;
         P.d_ntiles = (int *)q; q += s_nt;
         P.d_ctl = (int *)q; q += s_ctl;
-        P.d_gitems = (BatchItem *)q;
+        P.d_gitems = (BatchItem *)q; q += s_gitems;
+        P.d_xitems = (XGroupItem *)q;
         e = cudaMemcpy(P.d_items, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(P.d_passes, args.data(), args.size() * sizeof(PassArgs), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(P.d_binds, binds.data(), binds.size() * sizeof(PassBind), cudaMemcpyHostToDevice);
@@ -416,10 +468,12 @@ int build_plan(fftb_batch_s *b, int op, double sign)
         if (e == cudaSuccess) e = cudaMemset(P.d_ctl, 0, (2 + P.npasses) * sizeof(int));
         if (e == cudaSuccess)
             e = cudaMemcpy(P.d_gitems, gitems.data(), gitems.size() * sizeof(BatchItem), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !xitems.empty())
+            e = cudaMemcpy(P.d_xitems, xitems.data(), xitems.size() * sizeof(XGroupItem), cudaMemcpyHostToDevice);
         // the limit is per kernel, not per plan: raise it to the maximum once, so a later
         // plan with a smaller need cannot lower it under an earlier plan's launches
         for (const OpPlan::Group &g : P.groups)
-            if (e == cudaSuccess && g.smem > 48 * 1024) e = raise_smem_limit(batch_group_fn(g.nf));
+            if (e == cudaSuccess && !g.xcol && g.smem > 48 * 1024) e = raise_smem_limit(batch_group_fn(g.nf));
         if (e != cudaSuccess) return set_status_from_cuda(e);
         if (smem > 48 * 1024) {
             e = raise_smem_limit((const void *)batch_persistent_kernel);
@@ -452,6 +506,13 @@ int launch_persistent(OpPlan &P, const void *in, void *out, void *work, cudaStre
 int launch_groups(OpPlan &P, const void *in, void *out, void *work, cudaStream_t s)
 {
     for (const OpPlan::Group &g : P.groups) {
+        if (g.xcol) {
+            void *data = g.buf == B_IN ? const_cast<void *>(in) : (g.buf == B_OUT ? out : work);
+            int st = launch_col_group(g.ckind, g.nf, P.d_xitems + g.offset, g.count, data, g.roots, g.ep_mode,
+                                      g.ep_scale, g.ep_sign, s);
+            if (st != FFTB_SUCCESS) return st;
+            continue;
+        }
         const BatchItem *items = P.d_gitems + g.offset;
         const PassArgs *passes = P.d_passes;
         const PassBind *binds = P.d_binds;

@@ -369,7 +369,8 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
                     v[r] = mk<R>(h0.x - hn.y, h0.y + hn.x);
                 }
             }
-            __syncthreads();  // this block's columns (and the packed partners) are read
+            // no barrier: each group writes back only its own slot column, and the packed
+            // slot's partners (column 0, its own, and the kz = NZ/2 column) are never written
             regfft_warp_rt<R, NY, +1>(v, reg, twy, t);
             if (ok) {
 #pragma unroll
@@ -649,10 +650,11 @@ template <typename R> __device__ __forceinline__ void xcol_halfw(cpx<R> (&v)[16]
 // 4: inverse of 3: reads the rows tin[col][kx], writes the columns in place of `data`.
 // blockIdx.y selects a batch of column sets `bstride` elements apart (the transposed
 // side has NX * ncols elements per batch).
+// The body of one column tile (blockIdx.x of xcol_kernel): tile `tile` of batch `batch`.
 template <typename R, int NX, int MODE, bool TC>
-__global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data, long long stride, int ncols,
-                                                   long long bstride, cpx<R> *__restrict__ tdata,
-                                                   const cpx<R> *__restrict__ roots, XColEp ep)
+__device__ __forceinline__ void xcol_tile(cpx<R> *__restrict__ data, long long stride, int ncols, long long bstride,
+                                          cpx<R> *__restrict__ tdata, const cpx<R> *__restrict__ roots,
+                                          const XColEp &ep, int tile, int batch)
 {
     using C = cpx<R>;
     constexpr int T = XColShape<NX>::T, W = XColShape<NX>::W;
@@ -667,15 +669,15 @@ __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data,
     const int tid = threadIdx.x;
     const int t = tid / W, col = tid - (tid / W) * W;
     for (int i = tid; i < NX; i += 256) tw[i] = roots[i];
-    const int cg0 = blockIdx.x * W + col;
+    const int cg0 = tile * W + col;
     const bool ok = cg0 < ncols;
-    data += (size_t)blockIdx.y * bstride;
+    data += (size_t)batch * bstride;
     C *p = data + (ok ? cg0 : 0);
     C v[16];
     if (MODE == 4) {
         // rows of the transposed input -> shared memory -> columns in registers
-        const C *src = tdata + (size_t)blockIdx.y * NX * ncols + (size_t)blockIdx.x * W * NX;
-        const int nrow = (ncols - (int)blockIdx.x * W) < W ? (ncols - (int)blockIdx.x * W) : W;
+        const C *src = tdata + (size_t)batch * NX * ncols + (size_t)tile * W * NX;
+        const int nrow = (ncols - tile * W) < W ? (ncols - tile * W) : W;
         // all of the tile's row loads in flight at once
         for (int e = tid; e < nrow * NX; e += 256) {
             const int rr = e / NX, kx = e - (e / NX) * NX;
@@ -703,19 +705,81 @@ __global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data,
 #pragma unroll
         for (int j = 0; j < 16; ++j) scr[col * RP + t + T * j] = v[j];
         __syncthreads();
-        C *dstp = tdata + (size_t)blockIdx.y * NX * ncols + (size_t)blockIdx.x * W * NX;
-        const int nrow = (ncols - (int)blockIdx.x * W) < W ? (ncols - (int)blockIdx.x * W) : W;
+        C *dstp = tdata + (size_t)batch * NX * ncols + (size_t)tile * W * NX;
+        const int nrow = (ncols - tile * W) < W ? (ncols - tile * W) : W;
         for (int e = tid; e < nrow * NX; e += 256) {
             const int rr = e / NX, kx = e - (e / NX) * NX;
             dstp[(size_t)rr * NX + kx] = scr[rr * RP + kx];
         }
     } else if (ok) {
-        C *q = (MODE == 2 && tdata) ? tdata + (size_t)blockIdx.y * bstride + cg0 : p;
+        C *q = (MODE == 2 && tdata) ? tdata + (size_t)batch * bstride + cg0 : p;
 #pragma unroll
         for (int j = 0; j < 16; ++j) q[(size_t)(t + T * j) * stride] = v[j];
     }
 }
 
+template <typename R, int NX, int MODE, bool TC>
+__global__ void __launch_bounds__(256, 3) xcol_kernel(cpx<R> *__restrict__ data, long long stride, int ncols,
+                                                   long long bstride, cpx<R> *__restrict__ tdata,
+                                                   const cpx<R> *__restrict__ roots, XColEp ep)
+{
+    xcol_tile<R, NX, MODE, TC>(data, stride, ncols, bstride, tdata, roots, ep, (int)blockIdx.x, (int)blockIdx.y);
+}
+
+// One launch over the column tiles of many 3D spectra of one x length (the batched
+// transforms' x stage; MODE 0 forward, 1 inverse, 2 sandwich): item i is tile items[i].tile of
+// the spectrum at data + items[i].off with ny * (nz/2 + 1) columns; the spectral multiply
+// takes that spectrum's ny and nz.
+template <int NX, int MODE>
+__global__ void __launch_bounds__(256, 2) xcol_group_kernel(const XGroupItem *__restrict__ items,
+                                                         float2 *__restrict__ data,
+                                                         const float2 *__restrict__ roots, XColEp ep)
+{
+    const XGroupItem it = items[blockIdx.x];
+    ep.ny = it.ny;
+    ep.nz = it.nz;
+    ep.nzh = it.nz / 2 + 1;
+    ep.hn = it.nz;
+    xcol_tile<float, NX, MODE, false>(data + it.off, it.ncols, it.ncols, 0, nullptr, roots, ep, it.tile, 0);
+}
+
+// The y FFT (MODE 0 forward, 1 inverse) of many 3D spectra [nx][ny][nzh] of one y length in
+// one launch: the lines (x, kz) of a spectrum, kz fastest, in tiles of W lines, so a warp
+// reads 32 consecutive lines of a y row (contiguous within each x); the FFT is the column
+// kernel's register-resident one.  items[i].ncols holds nx * nzh (the lines), .tile the
+// tile, .ny / .nz the spectrum's sizes.
+template <int NY, int MODE>
+__global__ void __launch_bounds__(256, 2) ycol_group_kernel(const XGroupItem *__restrict__ items,
+                                                         float2 *__restrict__ data,
+                                                         const float2 *__restrict__ roots)
+{
+    using C = float2;
+    constexpr int T = XColShape<NY>::T, W = XColShape<NY>::W;
+    constexpr int RP = NY + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *scr = reinterpret_cast<C *>(smem_raw);
+    C *tw = scr + (16 * T * W > W * RP ? 16 * T * W : W * RP);
+    const XGroupItem it = items[blockIdx.x];
+    const int tid = threadIdx.x;
+    const int t = tid / W, col = tid - (tid / W) * W;
+    for (int i = tid; i < NY; i += 256) tw[i] = roots[i];
+    const int nzh = it.nz / 2 + 1;
+    const int l = it.tile * W + col;
+    const bool ok = l < it.ncols;
+    const int lc = ok ? l : 0;
+    const int x = lc / nzh, kz = lc - (lc / nzh) * nzh;
+    C *p = data + it.off + (long long)x * it.ny * nzh + kz;
+    C v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = p[(size_t)(t + T * r) * nzh];
+    __syncthreads();
+    TcDft16 F;
+    xcol_fft<float, NY, MODE == 1 ? +1 : -1, false>(v, scr, tw, t, col, nullptr, F);
+    if (ok) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) p[(size_t)(t + T * j) * nzh] = v[j];
+    }
+}
 // ------------------------------------------------------------------ x column kernel, TMA ring
 // Persistent form of xcol_kernel (MODE 0, 1, 2) for 16-byte aligned spectra: each CTA walks
 // the tiles (W columns x NX rows; blockIdx.x, + gridDim.x, ...) with NSTAGE tiles in flight,
@@ -1107,6 +1171,65 @@ int launch_xcol(const Fused3D &f, int mode, void *data, const EpValues *ep, cuda
 }
 
 } // namespace
+
+namespace {
+// kind: 0 x forward, 1 x inverse, 2 x sandwich, 3 y forward, 4 y inverse
+const void *col_group_fn(int kind, int n)
+{
+#define FFTB_COLG(N)                                                                                                   \
+    case N:                                                                                                            \
+        return kind == 0   ? (const void *)&xcol_group_kernel<N, 0>                                                    \
+               : kind == 1 ? (const void *)&xcol_group_kernel<N, 1>                                                    \
+               : kind == 2 ? (const void *)&xcol_group_kernel<N, 2>                                                    \
+               : kind == 3 ? (const void *)&ycol_group_kernel<N, 0>                                                    \
+                           : (const void *)&ycol_group_kernel<N, 1>;
+    if (kind < 0 || kind > 4) return nullptr;
+    switch (n) {
+        FFTB_COLG(32)
+        FFTB_COLG(64)
+        FFTB_COLG(128)
+        FFTB_COLG(256)
+    default:
+        return nullptr;
+    }
+#undef FFTB_COLG
+}
+} // namespace
+
+int col_group_tile_lines(int dtype, int n)
+{
+    return dtype == FFTB_F32 && col_group_fn(0, n) && find_xcol(dtype, n) ? 256 / (n / 16) : 0;
+}
+
+int col_group_prepare(int dtype, int kind, int n, void **roots)
+{
+    const XColEntry *e = find_xcol(dtype, n);
+    if (!e || !col_group_fn(kind, n)) return FFTB_ERROR_UNSUPPORTED_SIZE;
+    int st = configure(col_group_fn(kind, n), e->smem);
+    if (st != FFTB_SUCCESS) return st;
+    return engine_roots(dtype, n, roots);
+}
+
+int launch_col_group(int kind, int n, const XGroupItem *items, int nitems, void *data, const void *roots,
+                     int ep_mode, double scale, double sign, cudaStream_t s)
+{
+    const XColEntry *e = find_xcol(FFTB_F32, n);
+    const void *fn = col_group_fn(kind, n);
+    if (!e || !fn || nitems <= 0) return FFTB_ERROR_INVALID_VALUE;
+    float2 *d = (float2 *)data;
+    const float2 *rt = (const float2 *)roots;
+    if (kind >= 3) {
+        void *args[] = {&items, &d, &rt};
+        return set_status_from_cuda(cudaLaunchKernel(fn, dim3((unsigned)nitems), dim3(256), args, e->smem, s));
+    }
+    EpValues ev;
+    ev.mode = ep_mode;
+    ev.scale = scale;
+    ev.sign = sign;
+    XColEp x = make_ep(&ev);
+    void *args[] = {&items, &d, &rt, &x};
+    return set_status_from_cuda(cudaLaunchKernel(fn, dim3((unsigned)nitems), dim3(256), args, e->smem, s));
+}
 
 int fused3d_clusters(int dtype, long long nx, long long ny, long long nz, int *clusters, int cap)
 {

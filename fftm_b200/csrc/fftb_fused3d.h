@@ -42,6 +42,24 @@ int fused3d_gradient(const Fused3D &f, const void *in, void *spec, void *spec2, 
                      LaunchTimer *t);
 int fused3d_num_launches(const Fused3D &f, int which);
 
+// The x or y FFTs of many f32 3D spectra [nx][ny][nz/2+1] of one line length in one launch,
+// one CTA per tile of lines, with the column kernel's register-resident FFT (the batched
+// transforms' column stages).  kind: 0 x forward, 1 x inverse, 2 x sandwich (forward,
+// spectral multiply, inverse), 3 y forward, 4 y inverse.
+struct XGroupItem {
+    long long off;  // complex elements from the buffer base to the spectrum
+    int ncols;      // lines of the spectrum: x kinds ny * (nz/2 + 1), y kinds nx * (nz/2 + 1)
+    int tile;       // tile of col_group_tile_lines(n) lines
+    int ny, nz;
+};
+// 0 when no grouped column kernel exists for this line length, else the lines per tile
+int col_group_tile_lines(int dtype, int n);
+// Raises the kernel's shared-memory limit and returns the root table of length n.
+int col_group_prepare(int dtype, int kind, int n, void **roots);
+// ep_mode / scale / sign: the sandwich's multiply (EP_SCALE, EP_POISSON as the pass epilogue)
+int launch_col_group(int kind, int n, const XGroupItem *items, int nitems, void *data, const void *roots,
+                     int ep_mode, double scale, double sign, cudaStream_t s);
+
 // 4D slab / native_xzwy with power-of-two (z, w) planes and x, y column kernels.
 struct Fused4D {
     bool enabled = false;

@@ -69,18 +69,24 @@ def test_batch_roundtrip_poisson_modes_agree(B, torch_cuda):
             torch.cuda.synchronize()
             assert b.status(op) == 0
             outs[(op, mode)] = out.cpu().numpy()
-        # the same per-line arithmetic in every mode
-        for mode in (1, 2, 3, 4):
+        # the same per-line arithmetic in the sequential and persistent modes, and between
+        # the two grouped modes; the grouped modes run the x and y stages of the power-of-two
+        # lengths with the column kernel's FFT, so they agree with the others to rounding
+        for mode in (1, 2):
             np.testing.assert_array_equal(outs[(op, 0)], outs[(op, mode)])
-    rt = outs[(B.ROUNDTRIP, 2)].astype(np.float64)
-    assert O.rel_l2(rt, host.astype(np.float64)) <= TOL
-    po = outs[(B.POISSON, 2)].astype(np.float64)
-    for i in (0, 7, 21, 39):
-        s = shapes[i]
-        o = b.real_offsets[i]
-        n = int(np.prod(s))
-        ref = O.poisson3d_solve(host[o:o + n].reshape(s).astype(np.float64), -1.0)
-        assert O.rel_l2(po[o:o + n].reshape(s), ref) <= TOL
+        np.testing.assert_array_equal(outs[(op, 3)], outs[(op, 4)])
+        d = O.rel_l2(outs[(op, 4)].astype(np.float64), outs[(op, 0)].astype(np.float64))
+        assert d <= 1e-6, d
+    for mode in (2, 4):
+        rt = outs[(B.ROUNDTRIP, mode)].astype(np.float64)
+        assert O.rel_l2(rt, host.astype(np.float64)) <= TOL
+        po = outs[(B.POISSON, mode)].astype(np.float64)
+        for i in (0, 7, 21, 39):
+            s = shapes[i]
+            o = b.real_offsets[i]
+            n = int(np.prod(s))
+            ref = O.poisson3d_solve(host[o:o + n].reshape(s).astype(np.float64), -1.0)
+            assert O.rel_l2(po[o:o + n].reshape(s), ref) <= TOL
 
 
 def test_batch_full_workload_512(B, torch_cuda):
