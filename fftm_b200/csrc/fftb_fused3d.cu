@@ -536,8 +536,8 @@ struct XColEp {
 
 template <int NX> struct XColShape {
     static constexpr int T = RegFFTShape<NX>::T;
-    static constexpr int W = 256 / T;      // columns per CTA
-    static constexpr int NT = 256;
+    static constexpr int W = 256 / T;      // columns per CTA (48, 96 points: T = 3, 6, and the
+    static constexpr int NT = 256;         // threads past T * W idle)
 };
 
 // TC: the first radix-16 stage runs on the tensor cores (fftb_tc.cuh, float only)
@@ -547,6 +547,46 @@ __device__ __forceinline__ void xcol_fft(cpx<R> (&v)[16], cpx<R> *scr, const cpx
 {
     using C = cpx<R>;
     constexpr int T = XColShape<NX>::T, W = XColShape<NX>::W;
+    if constexpr (16 % T != 0) {
+        // T = 3 or 6 threads per column (48 or 96 points): thread t runs the second-stage DFTs
+        // of k1 = t, t + T, ... < 16, and one more exchange brings the results back to the
+        // layout v[j] = X[t + T j]; threads past T * W (t = T) take part in the barriers only
+        static_assert(!TC, "tensor-core form: power-of-two columns only");
+        const bool act = t < T;
+        const int tt = act ? t : 0;
+        dft16<SIGN, C, R>(v);
+#pragma unroll
+        for (int k1 = 1; k1 < 16; ++k1) v[k1] = twiddle_mul<SIGN>(v[k1], tw, tt * k1);
+        __syncthreads();
+        if (act) {
+#pragma unroll
+            for (int k1 = 0; k1 < 16; ++k1) scr[(k1 * T + t) * W + col] = v[k1];
+        }
+        __syncthreads();
+        constexpr int A = (16 + T - 1) / T;
+        C res[A][T];
+#pragma unroll
+        for (int a = 0; a < A; ++a) {
+            const int k1 = tt + T * a;
+            const bool valid = act && k1 < 16;
+#pragma unroll
+            for (int q = 0; q < T; ++q) res[a][q] = valid ? scr[(k1 * T + q) * W + col] : mk<R>(R(0), R(0));
+            dft_small<SIGN, T, C, R>(res[a]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < A; ++a) {
+            const int k1 = tt + T * a;
+            if (act && k1 < 16) {
+#pragma unroll
+                for (int k2 = 0; k2 < T; ++k2) scr[(k1 + 16 * k2) * W + col] = res[a][k2];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = act ? scr[(t + T * j) * W + col] : mk<R>(R(0), R(0));
+        return;
+    }
     if constexpr (TC) tc_dft16<SIGN>(v, stage, F, (int)(threadIdx.x & 31));
     else dft16<SIGN, C, R>(v);
 #pragma unroll
@@ -670,7 +710,8 @@ __device__ __forceinline__ void xcol_tile(cpx<R> *__restrict__ data, long long s
     const int t = tid / W, col = tid - (tid / W) * W;
     for (int i = tid; i < NX; i += 256) tw[i] = roots[i];
     const int cg0 = tile * W + col;
-    const bool ok = cg0 < ncols;
+    const bool act = t < T;  // false only for the idle threads of 48- and 96-point columns
+    const bool ok = act && cg0 < ncols;
     data += (size_t)batch * bstride;
     C *p = data + (ok ? cg0 : 0);
     C v[16];
@@ -689,7 +730,7 @@ __device__ __forceinline__ void xcol_tile(cpx<R> *__restrict__ data, long long s
         for (int r = 0; r < 16; ++r) v[r] = scr[col * RP + t + T * r];
     } else {
 #pragma unroll
-        for (int r = 0; r < 16; ++r) v[r] = p[(size_t)(t + T * r) * stride];
+        for (int r = 0; r < 16; ++r) v[r] = act ? p[(size_t)(t + T * r) * stride] : mk<R>(R(0), R(0));
     }
     __syncthreads();
     if (MODE == 1 || MODE == 4) xcol_fft<R, NX, +1, TC>(v, scr, tw, t, col, stage, F);
@@ -765,13 +806,14 @@ __global__ void __launch_bounds__(256, 2) ycol_group_kernel(const XGroupItem *__
     for (int i = tid; i < NY; i += 256) tw[i] = roots[i];
     const int nzh = it.nz / 2 + 1;
     const int l = it.tile * W + col;
-    const bool ok = l < it.ncols;
+    const bool act = t < T;  // false only for the idle threads of 48- and 96-point lines
+    const bool ok = act && l < it.ncols;
     const int lc = ok ? l : 0;
     const int x = lc / nzh, kz = lc - (lc / nzh) * nzh;
     C *p = data + it.off + (long long)x * it.ny * nzh + kz;
     C v[16];
 #pragma unroll
-    for (int r = 0; r < 16; ++r) v[r] = p[(size_t)(t + T * r) * nzh];
+    for (int r = 0; r < 16; ++r) v[r] = act ? p[(size_t)(t + T * r) * nzh] : mk<float>(0.f, 0.f);
     __syncthreads();
     TcDft16 F;
     xcol_fft<float, NY, MODE == 1 ? +1 : -1, false>(v, scr, tw, t, col, nullptr, F);
@@ -1186,7 +1228,9 @@ const void *col_group_fn(int kind, int n)
     if (kind < 0 || kind > 4) return nullptr;
     switch (n) {
         FFTB_COLG(32)
+        FFTB_COLG(48)
         FFTB_COLG(64)
+        FFTB_COLG(96)
         FFTB_COLG(128)
         FFTB_COLG(256)
     default:
@@ -1194,18 +1238,25 @@ const void *col_group_fn(int kind, int n)
     }
 #undef FFTB_COLG
 }
+
+// dynamic shared memory of a column tile: the exchange / transposing area and the root table
+size_t col_group_smem(int n)
+{
+    const int T = n / 16, W = 256 / T;
+    const size_t scr = (size_t)16 * T * W > (size_t)W * (n + 1) ? (size_t)16 * T * W : (size_t)W * (n + 1);
+    return sizeof(float2) * (scr + (size_t)n);
+}
 } // namespace
 
 int col_group_tile_lines(int dtype, int n)
 {
-    return dtype == FFTB_F32 && col_group_fn(0, n) && find_xcol(dtype, n) ? 256 / (n / 16) : 0;
+    return dtype == FFTB_F32 && col_group_fn(0, n) ? 256 / (n / 16) : 0;
 }
 
 int col_group_prepare(int dtype, int kind, int n, void **roots)
 {
-    const XColEntry *e = find_xcol(dtype, n);
-    if (!e || !col_group_fn(kind, n)) return FFTB_ERROR_UNSUPPORTED_SIZE;
-    int st = configure(col_group_fn(kind, n), e->smem);
+    if (dtype != FFTB_F32 || !col_group_fn(kind, n)) return FFTB_ERROR_UNSUPPORTED_SIZE;
+    int st = configure(col_group_fn(kind, n), col_group_smem(n));
     if (st != FFTB_SUCCESS) return st;
     return engine_roots(dtype, n, roots);
 }
@@ -1213,14 +1264,14 @@ int col_group_prepare(int dtype, int kind, int n, void **roots)
 int launch_col_group(int kind, int n, const XGroupItem *items, int nitems, void *data, const void *roots,
                      int ep_mode, double scale, double sign, cudaStream_t s)
 {
-    const XColEntry *e = find_xcol(FFTB_F32, n);
     const void *fn = col_group_fn(kind, n);
-    if (!e || !fn || nitems <= 0) return FFTB_ERROR_INVALID_VALUE;
+    if (!fn || nitems <= 0) return FFTB_ERROR_INVALID_VALUE;
+    const size_t smem = col_group_smem(n);
     float2 *d = (float2 *)data;
     const float2 *rt = (const float2 *)roots;
     if (kind >= 3) {
         void *args[] = {&items, &d, &rt};
-        return set_status_from_cuda(cudaLaunchKernel(fn, dim3((unsigned)nitems), dim3(256), args, e->smem, s));
+        return set_status_from_cuda(cudaLaunchKernel(fn, dim3((unsigned)nitems), dim3(256), args, smem, s));
     }
     EpValues ev;
     ev.mode = ep_mode;
@@ -1228,7 +1279,7 @@ int launch_col_group(int kind, int n, const XGroupItem *items, int nitems, void 
     ev.sign = sign;
     XColEp x = make_ep(&ev);
     void *args[] = {&items, &d, &rt, &x};
-    return set_status_from_cuda(cudaLaunchKernel(fn, dim3((unsigned)nitems), dim3(256), args, e->smem, s));
+    return set_status_from_cuda(cudaLaunchKernel(fn, dim3((unsigned)nitems), dim3(256), args, smem, s));
 }
 
 int fused3d_clusters(int dtype, long long nx, long long ny, long long nz, int *clusters, int cap)
