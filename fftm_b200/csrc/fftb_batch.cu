@@ -224,6 +224,8 @@ struct OpPlan {
         // x and y stages of lengths with a column kernel: one grouped column-kernel launch
         // over count tiles (XGroupItem offset ..) instead of the pass items
         bool xcol = false;
+        bool zrow = false;    // z stage as one grouped row-pair launch (RowGroupItem offset ..)
+        int in_buf = B_IN, out_buf = B_OUT;
         int ckind = 0;        // col_group kind: 0/1/2 x forward / inverse / sandwich, 3/4 y
         int buf = B_WORK;     // the buffer holding the spectra (in place)
         void *roots = nullptr;
@@ -233,6 +235,7 @@ struct OpPlan {
     std::vector<Group> groups;
     BatchItem *d_gitems = nullptr;
     XGroupItem *d_xitems = nullptr;
+    RowGroupItem *d_ritems = nullptr;
     // CUDA graph of the persistent launch (mode 2) or of the grouped launches (mode 4)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -383,6 +386,7 @@ int build_plan(fftb_batch_s *b, int op, double sign)
     // each (the fused 3D path's register-resident column FFT, tiles of W lines)
     std::vector<BatchItem> gitems;
     std::vector<XGroupItem> xitems;
+    std::vector<RowGroupItem> ritems;
     gitems.reserve(items.size());
     for (int s = 0; s < P.nstages; ++s) {
         std::vector<int> nfs;
@@ -403,10 +407,50 @@ int build_plan(fftb_batch_s *b, int op, double sign)
                                                 : (a0.is == nzh0 ? (a0.kind == K_C2C_FWD ? 3 : 4) : -1);
             }
         }
+        // z stages: R2C of contiguous real rows (no epilogue) or scaled C2R back to them
+        int zdir = -1;
+        {
+            const Launch &L0 = P.seq.launches[tpass[0][s]];
+            const PassArgs &a0 = L0.args;
+            if (b->dtype == FFTB_F32 && L0.longline == nullptr && a0.bs_n == 0 && a0.half && a0.is == 1 &&
+                a0.os == 1) {
+                if (a0.kind == K_R2C && a0.ep_mode == 0) zdir = 0;
+                else if (a0.kind == K_C2R && (a0.ep_mode & ~EP_SCALE) == 0) zdir = 1;
+            }
+        }
         for (int nf : nfs) {
+            // nf is the half length for the z stages: the row length is 2 nf
+            const int FZ = zdir >= 0 ? row_group_tile_pairs(b->dtype, 2 * nf) : 0;
+            if (FZ > 0) {
+                OpPlan::Group g{(int)ritems.size(), 0, nf, 0};
+                g.zrow = true;
+                const Launch &L0 = P.seq.launches[tpass[0][s]];
+                g.in_buf = L0.in_buf;
+                g.out_buf = L0.out_buf;
+                g.ckind = zdir;
+                int st = row_group_prepare(b->dtype, zdir, 2 * nf, &g.roots);
+                if (st != FFTB_SUCCESS) return st;
+                for (int i = 0; i < b->count; ++i) {
+                    const long long nx = b->dims[3 * i], ny = b->dims[3 * i + 1], nz = b->dims[3 * i + 2];
+                    if (nz != 2 * nf) continue;
+                    const Launch &L = P.seq.launches[tpass[i][s]];
+                    const long long roff = (long long)((zdir == 0 ? L.in_off_bytes : L.out_off_bytes) / real_bytes(b->dtype));
+                    const long long soff =
+                        (long long)((zdir == 0 ? L.out_off_bytes : L.in_off_bytes) / complex_bytes(b->dtype));
+                    const long long rows = nx * ny, pairs = (rows + 1) / 2;
+                    const float sc = zdir == 1 && (L.args.ep_mode & EP_SCALE) ? (float)L.args.ep_scale : 1.0f;
+                    for (long long t = 0; t < (pairs + FZ - 1) / FZ; ++t)
+                        ritems.push_back(RowGroupItem{roff, soff, (int)rows, (int)t, sc});
+                }
+                g.count = (int)ritems.size() - g.offset;
+                if (g.count > 0) P.groups.push_back(g);
+                continue;
+            }
             const int W = ckind >= 0 ? col_group_tile_lines(b->dtype, nf) : 0;
             if (W > 0) {
-                OpPlan::Group g{(int)xitems.size(), 0, nf, 0, true, ckind, B_WORK, nullptr};
+                OpPlan::Group g{(int)xitems.size(), 0, nf, 0};
+                g.xcol = true;
+                g.ckind = ckind;
                 const Launch &L0 = P.seq.launches[tpass[0][s]];
                 g.buf = L0.in_buf;
                 g.ep_mode = L0.args.ep_mode;
@@ -445,7 +489,8 @@ int build_plan(fftb_batch_s *b, int op, double sign)
                      s_nt = al(ntiles.size() * sizeof(int)), s_ctl = al((2 + P.npasses) * sizeof(int));
         const size_t s_gitems = al(gitems.size() * sizeof(BatchItem));
         const size_t s_xitems = al(xitems.size() * sizeof(XGroupItem));
-        const size_t tot = s_items + s_args + s_binds + s_deps + s_nt + s_ctl + s_gitems + s_xitems;
+        const size_t s_ritems = al(ritems.size() * sizeof(RowGroupItem));
+        const size_t tot = s_items + s_args + s_binds + s_deps + s_nt + s_ctl + s_gitems + s_xitems + s_ritems;
         cudaError_t e = cudaMalloc(&P.blob, tot);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -459,7 +504,8 @@ int build_plan(fftb_batch_s *b, int op, double sign)
         P.d_ntiles = (int *)q; q += s_nt;
         P.d_ctl = (int *)q; q += s_ctl;
         P.d_gitems = (BatchItem *)q; q += s_gitems;
-        P.d_xitems = (XGroupItem *)q;
+        P.d_xitems = (XGroupItem *)q; q += s_xitems;
+        P.d_ritems = (RowGroupItem *)q;
         e = cudaMemcpy(P.d_items, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(P.d_passes, args.data(), args.size() * sizeof(PassArgs), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(P.d_binds, binds.data(), binds.size() * sizeof(PassBind), cudaMemcpyHostToDevice);
@@ -470,10 +516,13 @@ int build_plan(fftb_batch_s *b, int op, double sign)
             e = cudaMemcpy(P.d_gitems, gitems.data(), gitems.size() * sizeof(BatchItem), cudaMemcpyHostToDevice);
         if (e == cudaSuccess && !xitems.empty())
             e = cudaMemcpy(P.d_xitems, xitems.data(), xitems.size() * sizeof(XGroupItem), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !ritems.empty())
+            e = cudaMemcpy(P.d_ritems, ritems.data(), ritems.size() * sizeof(RowGroupItem), cudaMemcpyHostToDevice);
         // the limit is per kernel, not per plan: raise it to the maximum once, so a later
         // plan with a smaller need cannot lower it under an earlier plan's launches
         for (const OpPlan::Group &g : P.groups)
-            if (e == cudaSuccess && !g.xcol && g.smem > 48 * 1024) e = raise_smem_limit(batch_group_fn(g.nf));
+            if (e == cudaSuccess && !g.xcol && !g.zrow && g.smem > 48 * 1024)
+                e = raise_smem_limit(batch_group_fn(g.nf));
         if (e != cudaSuccess) return set_status_from_cuda(e);
         if (smem > 48 * 1024) {
             e = raise_smem_limit((const void *)batch_persistent_kernel);
@@ -505,7 +554,14 @@ int launch_persistent(OpPlan &P, const void *in, void *out, void *work, cudaStre
 
 int launch_groups(OpPlan &P, const void *in, void *out, void *work, cudaStream_t s)
 {
+    const void *bufs[3] = {in, out, work};
     for (const OpPlan::Group &g : P.groups) {
+        if (g.zrow) {
+            int st = launch_row_group(g.ckind, 2 * g.nf, P.d_ritems + g.offset, g.count, bufs[g.in_buf],
+                                      const_cast<void *>(bufs[g.out_buf]), g.roots, s);
+            if (st != FFTB_SUCCESS) return st;
+            continue;
+        }
         if (g.xcol) {
             void *data = g.buf == B_IN ? const_cast<void *>(in) : (g.buf == B_OUT ? out : work);
             int st = launch_col_group(g.ckind, g.nf, P.d_xitems + g.offset, g.count, data, g.roots, g.ep_mode,

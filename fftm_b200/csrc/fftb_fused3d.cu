@@ -979,6 +979,106 @@ const PlaneEntry *find_plane(int dtype, int ny, int nz, int cl)
     return nullptr;
 }
 
+// ------------------------------------------------------------------ grouped z rows (batches)
+// The R2C (DIR 0) or C2R (DIR 1) of the contiguous z rows of many 3D transforms of one even z
+// length NZ in one launch, two real rows per complex NZ-point FFT (the plane kernels' z stage
+// without the plane): a group of TZ = NZ / 16 threads holds the row pair in registers, so the
+// rows go from HBM to registers and back with one exchange through shared memory for the
+// FFT.  R2C: z = a + i b, X_a[k] = (Z[k] + conj Z[-k]) / 2, X_b[k] = (Z[k] - conj Z[-k]) / 2i,
+// DC and Nyquist real.  C2R: Z = X_a + i X_b over the Hermitian extension (the imaginary
+// parts of DC and Nyquist ignored, as the C2R pass does), a = Re IFFT(Z), b = Im IFFT(Z),
+// times the item's scale.  Item i: pair tile items[i].tile of the nrows rows at real
+// offset roff and spectrum offset soff.
+template <int NZ, int DIR>
+__global__ void __launch_bounds__(256) row_group_kernel(const RowGroupItem *__restrict__ items,
+                                                        const void *__restrict__ in, void *__restrict__ out,
+                                                        const float2 *__restrict__ roots)
+{
+    using C = float2;
+    constexpr int TZ = NZ / 16, FZ = 256 / TZ, NH = NZ / 2 + 1;
+    static_assert(NZ >= 32 && NZ <= 256 && (NZ & (NZ - 1)) == 0, "power-of-two rows of 32-256 points");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const RowGroupItem it = items[blockIdx.x];
+    const int tid = threadIdx.x;
+    const int f = tid / TZ, t = tid - (tid / TZ) * TZ;
+    C *reg = reinterpret_cast<C *>(smem_raw) + f * RegFFTShape<NZ>::REGION;
+    C tw[16];
+    load_stage_twiddles<float, NZ>(tw, roots, NZ, t);
+    const long long p = (long long)it.tile * FZ + f;  // row pair
+    const bool ok = 2 * p < it.nrows;
+    const bool hasb = 2 * p + 1 < it.nrows;
+    const long long pa = ok ? 2 * p : 0, pb = hasb ? 2 * p + 1 : pa;
+    C v[16];
+    if constexpr (DIR == 0) {
+        const float *rin = reinterpret_cast<const float *>(in) + it.roff;
+        const float *ra = rin + pa * NZ, *rb = rin + pb * NZ;
+#pragma unroll
+        for (int r = 0; r < 16; ++r) v[r] = mk<float>(ra[t + TZ * r], hasb ? rb[t + TZ * r] : 0.f);
+        regfft_warp_rt<float, NZ, -1>(v, reg, tw, t);
+        // Z[t + TZ j] sits in lane t, register j; Z[NZ - (t + TZ j)] in lane (TZ - t) mod TZ,
+        // register 15 - j (t > 0), or in this lane, register (16 - j) mod 16 (t = 0)
+        const int lane = threadIdx.x & 31;
+        const int src = (lane - t) + ((TZ - t) & (TZ - 1));
+        const C zn = mk<float>(__shfl_sync(0xffffffffu, v[8].x, lane - t),
+                               __shfl_sync(0xffffffffu, v[8].y, lane - t));  // Z[NZ/2]
+        C *sout = reinterpret_cast<C *>(out) + it.soff;
+        C *oa = sout + pa * NH, *ob = sout + pb * NH;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int k = t + TZ * j;  // k < NZ/2
+            const C zk = v[j];
+            C zp;
+            zp.x = __shfl_sync(0xffffffffu, v[15 - j].x, src);
+            zp.y = __shfl_sync(0xffffffffu, v[15 - j].y, src);
+            if (t == 0) zp = v[(16 - j) & 15];
+            const C zm = cconj(zp);
+            C A = cscale(cadd(zk, zm), 0.5f);
+            C B = cscale(mul_si<-1>(csub(zk, zm)), 0.5f);
+            if (k == 0) {
+                A = mk<float>(zk.x, 0.f);
+                B = mk<float>(zk.y, 0.f);
+            }
+            if (ok) {
+                oa[k] = A;
+                if (hasb) ob[k] = B;
+            }
+        }
+        if (ok && t == 0) {
+            oa[NZ / 2] = mk<float>(zn.x, 0.f);
+            if (hasb) ob[NZ / 2] = mk<float>(zn.y, 0.f);
+        }
+    } else {
+        const C *sin_ = reinterpret_cast<const C *>(in) + it.soff;
+        const C *ha = sin_ + pa * NH, *hb = sin_ + pb * NH;
+        // n = t + TZ r: registers r < 8 hold n < NZ/2 (X[n]); r >= 8 hold n >= NZ/2, X[n] =
+        // conj X[NZ - n]; DC (r = 0) and Nyquist (r = 8) of lane t = 0 keep their real parts
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            const int k = r < 8 ? t + TZ * r : TZ * (16 - r) - t;
+            C xa = ha[k], xb = hasb ? hb[k] : mk<float>(0.f, 0.f);
+            if (r >= 8) {
+                xa = cconj(xa);
+                xb = cconj(xb);
+            }
+            if ((r == 0 || r == 8) && t == 0) {
+                xa.y = 0.f;
+                xb.y = 0.f;
+            }
+            v[r] = mk<float>(xa.x - xb.y, xa.y + xb.x);  // X_a + i X_b
+        }
+        regfft_warp_rt<float, NZ, +1>(v, reg, tw, t);
+        float *rout = reinterpret_cast<float *>(out) + it.roff;
+        float *ra = rout + pa * NZ, *rb = rout + pb * NZ;
+        if (ok) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                ra[t + TZ * j] = v[j].x * it.scale;
+                if (hasb) rb[t + TZ * j] = v[j].y * it.scale;
+            }
+        }
+    }
+}
+
 struct XColEntry {
     int dtype, nx;
     const void *fn[5];
@@ -1247,6 +1347,46 @@ size_t col_group_smem(int n)
     return sizeof(float2) * (scr + (size_t)n);
 }
 } // namespace
+
+namespace {
+const void *row_group_fn(int dir, int nz)
+{
+    switch (nz) {
+    case 32: return dir ? (const void *)&row_group_kernel<32, 1> : (const void *)&row_group_kernel<32, 0>;
+    case 64: return dir ? (const void *)&row_group_kernel<64, 1> : (const void *)&row_group_kernel<64, 0>;
+    case 128: return dir ? (const void *)&row_group_kernel<128, 1> : (const void *)&row_group_kernel<128, 0>;
+    case 256: return dir ? (const void *)&row_group_kernel<256, 1> : (const void *)&row_group_kernel<256, 0>;
+    default: return nullptr;
+    }
+}
+// one exchange region (RegFFTShape<nz>::REGION) per row-pair group
+size_t row_group_smem(int nz)
+{
+    const int T = nz / 16;
+    const int region = T == 1 ? 16 : 16 * (T + 1) + (T == 16 ? 0 : T);
+    return sizeof(float2) * (size_t)(256 / T) * region;
+}
+} // namespace
+
+int row_group_tile_pairs(int dtype, int nz) { return dtype == FFTB_F32 && row_group_fn(0, nz) ? 256 / (nz / 16) : 0; }
+
+int row_group_prepare(int dtype, int dir, int nz, void **roots)
+{
+    if (dtype != FFTB_F32 || !row_group_fn(dir, nz)) return FFTB_ERROR_UNSUPPORTED_SIZE;
+    int st = configure(row_group_fn(dir, nz), row_group_smem(nz));
+    if (st != FFTB_SUCCESS) return st;
+    return engine_roots(dtype, nz, roots);
+}
+
+int launch_row_group(int dir, int nz, const RowGroupItem *items, int nitems, const void *in, void *out,
+                     const void *roots, cudaStream_t s)
+{
+    const void *fn = row_group_fn(dir, nz);
+    if (!fn || nitems <= 0) return FFTB_ERROR_INVALID_VALUE;
+    const float2 *rt = (const float2 *)roots;
+    void *args[] = {&items, &in, &out, &rt};
+    return set_status_from_cuda(cudaLaunchKernel(fn, dim3((unsigned)nitems), dim3(256), args, row_group_smem(nz), s));
+}
 
 int col_group_tile_lines(int dtype, int n)
 {

@@ -60,6 +60,20 @@ int col_group_prepare(int dtype, int kind, int n, void **roots);
 int launch_col_group(int kind, int n, const XGroupItem *items, int nitems, void *data, const void *roots,
                      int ep_mode, double scale, double sign, cudaStream_t s);
 
+// The z stage of many f32 3D transforms of one z length (32-256, a power of two) in one launch:
+// R2C (dir 0) or scaled C2R (dir 1) of two contiguous real rows per complex FFT.
+struct RowGroupItem {
+    long long roff;  // floats from the real buffer base to the transform's rows [nrows][nz]
+    long long soff;  // complex elements from the spectrum buffer base to its rows [nrows][nz/2+1]
+    int nrows;       // rows (nx * ny)
+    int tile;        // tile of row_group_tile_pairs(nz) row pairs
+    float scale;     // C2R output scale
+};
+int row_group_tile_pairs(int dtype, int nz);
+int row_group_prepare(int dtype, int dir, int nz, void **roots);
+int launch_row_group(int dir, int nz, const RowGroupItem *items, int nitems, const void *in, void *out,
+                     const void *roots, cudaStream_t s);
+
 // 4D slab / native_xzwy with power-of-two (z, w) planes and x, y column kernels.
 struct Fused4D {
     bool enabled = false;

@@ -70,9 +70,9 @@ def test_batch_roundtrip_poisson_modes_agree(B, torch_cuda):
             assert b.status(op) == 0
             outs[(op, mode)] = out.cpu().numpy()
         # the same per-line arithmetic in the sequential and persistent modes, and between
-        # the two grouped modes; the grouped modes run the x and y stages with the column
-        # kernel's FFT (the same decomposition) and the Poisson multiply with a reciprocal,
-        # so they agree with the others to rounding
+        # the two grouped modes; the grouped modes run the column and z-row stages with the
+        # fused path's kernels (full-length complex z FFTs of row pairs, the Poisson multiply
+        # with a reciprocal), so they agree with the others to rounding
         for mode in (1, 2):
             np.testing.assert_array_equal(outs[(op, 0)], outs[(op, mode)])
         np.testing.assert_array_equal(outs[(op, 3)], outs[(op, 4)])
