@@ -23,11 +23,13 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <new>
 #include <string>
 #include <vector>
 
 #include "../../include/fftb.h"
+#include "fftb_coltile.cuh"
 #include "fftb_engine.h"
 #include "fftb_fused3d.h"
 #include "fftb_pass.cuh"
@@ -48,6 +50,14 @@ struct PassBind {
     int in_buf, out_buf;
     long long in_off, out_off;  // bytes
     int nf;
+    // the tile form of a pass on the fused path's kernels (f32): 0 the pass kernel's tile;
+    // 1 a column tile (ckind 0-2 x forward / inverse / sandwich, 3-4 y forward / inverse) of
+    // n-point lines; 2 a row-pair tile of n-point z rows (ckind 0 R2C, 1 C2R)
+    int fast, ckind, n;
+    int lines, ny, nz;      // column: lines of the spectrum, its ny and nz; row: rows
+    float scale, sign;      // row C2R scale; column sandwich scale and Poisson sign
+    int ep_mode;            // column sandwich multiply
+    const float2 *roots;    // n-point root table
 };
 
 __device__ __forceinline__ int ld_acquire(const int *p)
@@ -58,6 +68,40 @@ __device__ __forceinline__ int ld_acquire(const int *p)
 }
 
 #define FFTB_BATCH_NF_LIST(X) X(8) X(12) X(16) X(20) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(256)
+
+// Column and row-pair tiles of the persistent launch, one non-inlined function per kind and
+// length (their own register allocation, as the pass tiles have).
+template <int N, int KIND> __device__ __noinline__ void batch_col_tile(const PassBind *b, void *data, int tile)
+{
+    if constexpr (KIND <= 2) {
+        XColEp ep = {};
+        ep.mode = b->ep_mode;
+        ep.scale_f = b->scale;
+        ep.sign_f = b->sign;
+        ep.scale = b->scale;
+        ep.sign = b->sign;
+        ep.ny = b->ny;
+        ep.nz = b->nz;
+        ep.nzh = b->nz / 2 + 1;
+        ep.hn = b->nz;
+        ep.hw_f = 1.f;
+        ep.hw = 1.0;
+        xcol_tile<float, N, KIND, false>(reinterpret_cast<float2 *>(data), b->lines, b->lines, 0, nullptr, b->roots, ep,
+                                         tile, 0);
+    } else {
+        const XGroupItem it{0, b->lines, tile, b->ny, b->nz};
+        ycol_tile<N, KIND - 3>(it, reinterpret_cast<float2 *>(data), b->roots);
+    }
+}
+template <int N, int DIR>
+__device__ __noinline__ void batch_row_tile(const PassBind *b, const void *in, void *out, int tile)
+{
+    const RowGroupItem it{0, 0, b->lines, tile, b->scale};
+    row_tile<N, DIR>(it, in, out, b->roots);
+}
+
+#define FFTB_BATCH_COL_LIST(X) X(32) X(48) X(64) X(96) X(128) X(256)
+#define FFTB_BATCH_ROW_LIST(X) X(64) X(128) X(256)
 
 // One tile of a pass of line length NF; not inlined, so every length keeps its own
 // register allocation instead of the union of all of them.  The tile stages its lines
@@ -114,15 +158,41 @@ __global__ void __launch_bounds__(kBatchThreads)
         const void *pin = (const char *)bufs[b.in_buf] + b.in_off;
         void *pout = (char *)const_cast<void *>(bufs[b.out_buf]) + b.out_off;
         const long long line0 = (long long)bi.tile * a->G;
-        switch (b.nf) {
+        if (b.fast == 1) {
+            void *data = const_cast<void *>(pin);
+            switch (b.n * 8 + b.ckind) {
+#define FFTB_CCASE(n)                                                                                                 \
+    case n * 8 + 0: batch_col_tile<n, 0>(&binds[bi.pass], data, bi.tile); break;                                     \
+    case n * 8 + 1: batch_col_tile<n, 1>(&binds[bi.pass], data, bi.tile); break;                                     \
+    case n * 8 + 2: batch_col_tile<n, 2>(&binds[bi.pass], data, bi.tile); break;                                     \
+    case n * 8 + 3: batch_col_tile<n, 3>(&binds[bi.pass], data, bi.tile); break;                                     \
+    case n * 8 + 4: batch_col_tile<n, 4>(&binds[bi.pass], data, bi.tile); break;
+                FFTB_BATCH_COL_LIST(FFTB_CCASE)
+#undef FFTB_CCASE
+            default:
+                break;
+            }
+        } else if (b.fast == 2) {
+            switch (b.n * 2 + b.ckind) {
+#define FFTB_RCASE(n)                                                                                                 \
+    case n * 2 + 0: batch_row_tile<n, 0>(&binds[bi.pass], pin, pout, bi.tile); break;                                 \
+    case n * 2 + 1: batch_row_tile<n, 1>(&binds[bi.pass], pin, pout, bi.tile); break;
+                FFTB_BATCH_ROW_LIST(FFTB_RCASE)
+#undef FFTB_RCASE
+            default:
+                break;
+            }
+        } else {
+            switch (b.nf) {
 #define FFTB_CASE(n)                                                                                                  \
     case n:                                                                                                           \
         batch_tile<n>(a, pin, pout, line0, smem_raw);                                                                 \
         break;
-            FFTB_BATCH_NF_LIST(FFTB_CASE)
+                FFTB_BATCH_NF_LIST(FFTB_CASE)
 #undef FFTB_CASE
-        default:
-            break;
+            default:
+                break;
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -351,6 +421,35 @@ int build_plan(fftb_batch_s *b, int op, double sign)
     std::vector<int> deps(P.npasses, -1), ntiles(P.npasses, 0);
     size_t smem = 0;
     std::vector<size_t> pass_smem(P.npasses, 0);
+    // per stage: the column kind (x passes step C3 = ny * nzh between points, y passes nzh) or
+    // the z direction (R2C of contiguous real rows, scaled C2R back to them) of the stages the
+    // fused path's tiles can run (f32, in place for the column stages); the same for every
+    // transform, taken from the first
+    std::vector<int> st_ckind(P.nstages, -1), st_zdir(P.nstages, -1);
+    for (int s = 0; s < P.nstages; ++s) {
+        const Launch &L0 = P.seq.launches[tpass[0][s]];
+        const PassArgs &a0 = L0.args;
+        if (b->dtype != FFTB_F32 || L0.longline != nullptr || a0.bs_n != 0) continue;
+        const long long ny0 = b->dims[1], nzh0 = b->dims[2] / 2 + 1;
+        const bool inplace = L0.in_buf == L0.out_buf && L0.in_off_bytes == L0.out_off_bytes;
+        if (inplace && ny0 > 1) {
+            if (a0.kind == K_SANDWICH && a0.is == ny0 * nzh0) st_ckind[s] = 2;
+            else if ((a0.kind == K_C2C_FWD || a0.kind == K_C2C_INV) && a0.ep_mode == 0)
+                st_ckind[s] = a0.is == ny0 * nzh0 ? (a0.kind == K_C2C_FWD ? 0 : 1)
+                                                  : (a0.is == nzh0 ? (a0.kind == K_C2C_FWD ? 3 : 4) : -1);
+        }
+        if (a0.half && a0.is == 1 && a0.os == 1) {
+            if (a0.kind == K_R2C && a0.ep_mode == 0) st_zdir[s] = 0;
+            else if (a0.kind == K_C2R && (a0.ep_mode & ~EP_SCALE) == 0) st_zdir[s] = 1;
+        }
+    }
+    std::vector<int> stage_of(P.npasses, 0), trans_of(P.npasses, 0);
+    std::map<int, void *> roots_of;
+    for (int i = 0; i < b->count; ++i)
+        for (int s = 0; s < P.nstages; ++s) {
+            stage_of[tpass[i][s]] = s;
+            trans_of[tpass[i][s]] = i;
+        }
     for (int p = 0; p < P.npasses; ++p) {
         const Launch &L = P.seq.launches[p];
         PassArgs a = L.args;
@@ -368,8 +467,60 @@ int build_plan(fftb_batch_s *b, int op, double sign)
         smem = std::max(smem, sm);
         pass_smem[p] = sm;
         args[p] = a;
-        binds[p] = PassBind{L.in_buf, L.out_buf, (long long)L.in_off_bytes, (long long)L.out_off_bytes, L.k.nf};
+        PassBind pb = {};
+        pb.in_buf = L.in_buf;
+        pb.out_buf = L.out_buf;
+        pb.in_off = (long long)L.in_off_bytes;
+        pb.out_off = (long long)L.out_off_bytes;
+        pb.nf = L.k.nf;
         ntiles[p] = (int)((a.nlines + G - 1) / G);
+        // the fused path's tile for this pass, where the stage has one for this length
+        const int st = stage_of[p], ti = trans_of[p];
+        const long long nx = b->dims[3 * ti], ny = b->dims[3 * ti + 1], nz = b->dims[3 * ti + 2];
+        const int FZ = st_zdir[st] >= 0 ? row_group_tile_pairs(b->dtype, 2 * L.k.nf) : 0;
+        const int W = FZ == 0 && st_ckind[st] >= 0 ? col_group_tile_lines(b->dtype, L.k.nf) : 0;
+        void *roots = nullptr;
+        // the kernels' set-up (shared-memory limit, root table) once per kind and length
+        auto prepared = [&](int key, auto prepare) -> int {
+            auto it = roots_of.find(key);
+            if (it != roots_of.end()) {
+                roots = it->second;
+                return FFTB_SUCCESS;
+            }
+            int rs = prepare();
+            if (rs == FFTB_SUCCESS) roots_of[key] = roots;
+            return rs;
+        };
+        if (FZ > 0) {
+            int rs = prepared(100000 + st_zdir[st] * 1000 + 2 * L.k.nf,
+                              [&] { return row_group_prepare(b->dtype, st_zdir[st], 2 * L.k.nf, &roots); });
+            if (rs != FFTB_SUCCESS) return rs;
+            pb.fast = 2;
+            pb.ckind = st_zdir[st];
+            pb.n = 2 * L.k.nf;
+            pb.lines = (int)(nx * ny);
+            pb.scale = st_zdir[st] == 1 && (a.ep_mode & EP_SCALE) ? (float)a.ep_scale : 1.0f;
+            pb.roots = (const float2 *)roots;
+            ntiles[p] = (int)(((nx * ny + 1) / 2 + FZ - 1) / FZ);
+            smem = std::max(smem, row_group_smem(pb.n));
+        } else if (W > 0) {
+            int rs = prepared(st_ckind[st] * 1000 + L.k.nf,
+                              [&] { return col_group_prepare(b->dtype, st_ckind[st], L.k.nf, &roots); });
+            if (rs != FFTB_SUCCESS) return rs;
+            pb.fast = 1;
+            pb.ckind = st_ckind[st];
+            pb.n = L.k.nf;
+            pb.lines = (int)((st_ckind[st] <= 2 ? ny : nx) * (nz / 2 + 1));
+            pb.ny = (int)ny;
+            pb.nz = (int)nz;
+            pb.scale = (float)a.ep_scale;
+            pb.sign = (float)a.ep_sign;
+            pb.ep_mode = a.ep_mode;
+            pb.roots = (const float2 *)roots;
+            ntiles[p] = (pb.lines + W - 1) / W;
+            smem = std::max(smem, col_group_smem(pb.n));
+        }
+        binds[p] = pb;
     }
     for (int i = 0; i < b->count; ++i)
         for (int s = 1; s < P.nstages; ++s) deps[tpass[i][s]] = tpass[i][s - 1];
@@ -393,31 +544,7 @@ int build_plan(fftb_batch_s *b, int op, double sign)
         for (int i = 0; i < b->count; ++i) nfs.push_back(binds[tpass[i][s]].nf);
         std::sort(nfs.begin(), nfs.end());
         nfs.erase(std::unique(nfs.begin(), nfs.end()), nfs.end());
-        // the stage's column kind: x passes step C3 = ny * nzh between points, y passes nzh
-        int ckind = -1;
-        {
-            const Launch &L0 = P.seq.launches[tpass[0][s]];
-            const PassArgs &a0 = L0.args;
-            const long long ny0 = b->dims[1], nzh0 = b->dims[2] / 2 + 1;
-            const bool inplace = L0.in_buf == L0.out_buf && L0.in_off_bytes == L0.out_off_bytes;
-            if (b->dtype == FFTB_F32 && inplace && L0.longline == nullptr && a0.bs_n == 0 && ny0 > 1) {
-                if (a0.kind == K_SANDWICH && a0.is == ny0 * nzh0) ckind = 2;
-                else if ((a0.kind == K_C2C_FWD || a0.kind == K_C2C_INV) && a0.ep_mode == 0)
-                    ckind = a0.is == ny0 * nzh0 ? (a0.kind == K_C2C_FWD ? 0 : 1)
-                                                : (a0.is == nzh0 ? (a0.kind == K_C2C_FWD ? 3 : 4) : -1);
-            }
-        }
-        // z stages: R2C of contiguous real rows (no epilogue) or scaled C2R back to them
-        int zdir = -1;
-        {
-            const Launch &L0 = P.seq.launches[tpass[0][s]];
-            const PassArgs &a0 = L0.args;
-            if (b->dtype == FFTB_F32 && L0.longline == nullptr && a0.bs_n == 0 && a0.half && a0.is == 1 &&
-                a0.os == 1) {
-                if (a0.kind == K_R2C && a0.ep_mode == 0) zdir = 0;
-                else if (a0.kind == K_C2R && (a0.ep_mode & ~EP_SCALE) == 0) zdir = 1;
-            }
-        }
+        const int ckind = st_ckind[s], zdir = st_zdir[s];
         for (int nf : nfs) {
             // nf is the half length for the z stages: the row length is 2 nf
             const int FZ = zdir >= 0 ? row_group_tile_pairs(b->dtype, 2 * nf) : 0;

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstddef>
+
 #include "fftb_engine.h"
 
 namespace fftb {
@@ -70,6 +72,9 @@ struct RowGroupItem {
     float scale;     // C2R output scale
 };
 int row_group_tile_pairs(int dtype, int nz);
+// dynamic shared memory of one row-pair tile / one column tile
+size_t row_group_smem(int nz);
+size_t col_group_smem(int n);
 int row_group_prepare(int dtype, int dir, int nz, void **roots);
 int launch_row_group(int dir, int nz, const RowGroupItem *items, int nitems, const void *in, void *out,
                      const void *roots, cudaStream_t s);
