@@ -55,6 +55,49 @@ def test_batch_forward_backward_vs_oracle(B, torch_cuda, mode):
         assert O.rel_l2(res[o:o + n], host[o:o + n].astype(np.float64)) <= TOL, (i, s)
 
 
+# lengths with and without the fused path's column and row tiles side by side in one stage
+# (x, y: 32-128 column tiles, 8-40 the pass kernel; z: 64-256 row tiles, 16-96 the pass
+# kernel), and spectra with fewer lines than one tile
+EDGE_SHAPES = [(8, 12, 64), (12, 8, 128), (32, 20, 64), (64, 12, 128), (48, 16, 96), (96, 32, 40), (16, 16, 256),
+               (128, 8, 32), (20, 48, 128), (40, 96, 16)]
+
+
+@pytest.mark.parametrize("mode", [1, 2, 3, 4])
+def test_batch_edge_shapes_vs_oracle(B, torch_cuda, mode):
+    torch = torch_cuda
+    b = B.Batch(EDGE_SHAPES)
+    assert b.describe(B.ROUNDTRIP)["persistent"] == 1  # every length runs the one-launch forms
+    x, host = _fill(torch, b, 9)
+    spec = torch.zeros(b.spectrum_total, dtype=torch.complex64, device="cuda")
+    b.exec(B.FORWARD, x, spec, mode=mode)
+    torch.cuda.synchronize()
+    assert b.status(B.FORWARD) == 0
+    sp = spec.cpu().numpy().astype(np.complex128)
+    for i, s in enumerate(EDGE_SHAPES):
+        o = b.real_offsets[i]
+        xi = host[o:o + np.prod(s)].reshape(s).astype(np.float64)
+        so = b.spectrum_offsets[i]
+        got = sp[so:so + s[0] * s[1] * (s[2] // 2 + 1)].reshape(s[0], s[1], s[2] // 2 + 1)
+        assert O.rel_l2(got, O.ffts3d_forward(xi)) <= TOL, (i, s)
+    out = torch.zeros_like(x)
+    b.exec(B.ROUNDTRIP, x, out, mode=mode)
+    torch.cuda.synchronize()
+    res = out.cpu().numpy().astype(np.float64)
+    for i, s in enumerate(EDGE_SHAPES):
+        o = b.real_offsets[i]
+        n = int(np.prod(s))
+        assert O.rel_l2(res[o:o + n], host[o:o + n].astype(np.float64)) <= TOL, (i, s)
+    po = torch.zeros_like(x)
+    b.exec(B.POISSON, x, po, sign=-1.0, mode=mode)
+    torch.cuda.synchronize()
+    pr = po.cpu().numpy().astype(np.float64)
+    for i, s in enumerate(EDGE_SHAPES):
+        o = b.real_offsets[i]
+        n = int(np.prod(s))
+        ref = O.poisson3d_solve(host[o:o + n].reshape(s).astype(np.float64), -1.0)
+        assert O.rel_l2(pr[o:o + n].reshape(s), ref) <= TOL, (i, s)
+
+
 def test_batch_roundtrip_poisson_modes_agree(B, torch_cuda):
     torch = torch_cuda
     shapes = B.draw_shapes(40, seed=2)
