@@ -123,9 +123,16 @@ __global__ void __launch_bounds__(kBatchThreads)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item, s_ok;
+    // thread 0 takes the next item from the queue one item ahead, so the atomic's round trip
+    // overlaps the current item.  No deadlock: the unfinished item with the smallest index
+    // has all its producers finished (they come earlier in the stage order), and the CTA
+    // holding it either runs it or first finishes a current item with a smaller index.
+    int nxt = 0;
+    if (threadIdx.x == 0) nxt = atomicAdd(&ctl[0], 1);
     for (;;) {
         if (threadIdx.x == 0) {
-            const int it = atomicAdd(&ctl[0], 1);
+            const int it = nxt;
+            if (it < nitems) nxt = atomicAdd(&ctl[0], 1);
             int ok = 1;
             if (it < nitems) {
                 const int dp = deps[items[it].pass];
