@@ -176,15 +176,48 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
                 w[r].y = rb[t + TZ * r];
             }
         };
+        // One CTA per plane whose rows fit one round: the CTA's rows come in as row bulk copies
+        // (one per row, 16-byte aligned, pitch NZ + 4 floats so a warp's eight row pairs
+        // spread over the banks) into the plane buffer, which the pushes only fill after
+        // every row is read; the groups then read their row pairs from shared memory
+        constexpr int ZP = NZ + 4;
+        constexpr bool BULKZ = CL == 1 && sizeof(R) == 4 && S::M / 2 <= FZ && (NZ * sizeof(R)) % 16 == 0 &&
+                               (size_t)S::M * ZP * sizeof(R) <= (size_t)NY * S::PF * sizeof(C);
+        const bool bulkz = BULKZ && (reinterpret_cast<uintptr_t>(in) & 15) == 0;
+        if (BULKZ && bulkz) {
+            __shared__ __align__(8) unsigned long long zbar;
+            __shared__ int zok;
+            R *zst = reinterpret_cast<R *>(plane);
+            if (tid == 0) {
+                mbar_init(&zbar, 1);
+                mbar_init_fence();
+                mbar_arrive_expect_tx(&zbar, (unsigned)(S::M * NZ * sizeof(R)));
+            }
+            __syncthreads();  // the barrier exists before any copy completes on it
+            for (int row = tid; row < S::M; row += S::NT)
+                bulk_load(zst + row * ZP, rows + (size_t)row * NZ, (unsigned)(NZ * sizeof(R)), &zbar);
+            if (tid == 0) zok = mbar_wait(&zbar, 0, kRingWaitLimit) ? 1 : 0;
+            __syncthreads();
+            if (!zok) {  // a copy never completed: flag it and leave
+                if (tid == 0) atomicExch(&g_ring_wait_error, 4);
+                return;
+            }
+        }
         C nxt[16];
-        if (PREFETCH) load_rows(0, nxt);
+        if (PREFETCH && !bulkz) load_rows(0, nxt);
 #pragma unroll 1
         for (int p0 = 0; p0 < S::M / 2; p0 += FZ) {
             const int p = p0 + f;
             const bool ok = p < S::M / 2;
             const int pp = ok ? p : 0;
             C v[16];
-            if (PREFETCH) {
+            if (BULKZ && bulkz) {
+                const R *zst = reinterpret_cast<const R *>(plane);
+                const R *ra = zst + (2 * pp) * ZP, *rb = ra + ZP;
+#pragma unroll
+                for (int r = 0; r < 16; ++r) v[r] = mk<R>(ra[t + TZ * r], rb[t + TZ * r]);
+                __syncthreads();  // every staged row is read before the pushes overwrite it
+            } else if (PREFETCH) {
 #pragma unroll
                 for (int r = 0; r < 16; ++r) v[r] = nxt[r];
                 if (p0 + FZ < S::M / 2) load_rows(p0 + FZ, nxt);
