@@ -59,6 +59,17 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned b
                  : "memory");
 }
 
+// 1D bulk copy this CTA's shared memory -> global (16-byte aligned addresses, size a multiple
+// of 16) in the thread's bulk group; bulk_store_wait() waits for the thread's stores to finish
+__device__ __forceinline__ void bulk_store(void *dst, const void *src, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_store_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_store_wait() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+
 // ------------------------------------------------------------------ plane kernels
 // Work split (CL CTAs per plane, CL in {1, 2, 4, 8}):
 //   rows   : CTA c owns rows [c*M, (c+1)*M) for the z stage            (M = NY / CL)
@@ -500,6 +511,12 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
         load_stage_twiddles<R, NZ>(twz, roots, S::NMAX, t);
         C *reg = stg + f * RegFFTShape<NZ>::REGION;
         R *rows = out + ((size_t)x * NY + (size_t)c * S::M) * NZ;
+        // one CTA per plane, rows in one round: the real rows are collected in the staging
+        // area (pitch NZ + 4 floats) and leave as one bulk copy per row
+        constexpr int ZP = NZ + 4;
+        constexpr bool BULKS = CL == 1 && sizeof(R) == 4 && S::M / 2 <= FZ && (NZ * sizeof(R)) % 16 == 0 &&
+                               (size_t)S::M * ZP * sizeof(R) <= (size_t)S::STG * sizeof(C);
+        const bool bulks = BULKS && (reinterpret_cast<uintptr_t>(out) & 15) == 0;
 #pragma unroll 1
         for (int p0 = 0; p0 < S::M / 2; p0 += FZ) {
             const int p = p0 + f;
@@ -532,7 +549,25 @@ __global__ void __launch_bounds__(PlaneShape<NY, NZ, CL>::NT, PlaneShape<NY, NZ,
                 v[r] = mk<R>(ha.x - hb.y, ha.y + hb.x);  // Ha + i Hb
             }
             regfft_warp_rt<R, NZ, +1>(v, reg, twz, t);
-            if (ok) {
+            if (BULKS && bulks) {
+                R *zst = reinterpret_cast<R *>(stg);
+                __syncthreads();  // every group's FFT exchange in the staging area is done
+                if (ok) {
+                    R *ra = zst + (2 * pp) * ZP;
+                    R *rb = ra + ZP;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        ra[t + TZ * j] = v[j].x * scale;
+                        rb[t + TZ * j] = v[j].y * scale;
+                    }
+                }
+                fence_proxy_async_smem();  // the rows are visible to the bulk copies
+                __syncthreads();
+                for (int row = tid; row < S::M; row += S::NT)
+                    bulk_store(rows + (size_t)row * NZ, zst + row * ZP, (unsigned)(NZ * sizeof(R)));
+                bulk_store_commit();
+                bulk_store_wait();  // the staging area stays valid until the copies have read it
+            } else if (ok) {
                 R *ra = rows + (size_t)(2 * pp) * NZ;
                 R *rb = ra + NZ;
 #pragma unroll
