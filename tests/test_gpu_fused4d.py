@@ -108,3 +108,27 @@ def test_fused4d_tensor_core_form(F, torch_cuda, dims):
     err_p = O.rel_l2(_host(out), O.poisson4d_solve(O.NATIVE_XZWY, x, dims, -1.0))
     print(f"tensor-core form {dims}: forward {err_f:.2e}, round trip {err_rt:.2e}, Poisson {err_p:.2e}")
     assert err_f <= TC_TOL and err_rt <= TC_TOL and err_p <= TC_TOL
+
+
+def test_fused4d_unaligned_buffers(F, torch_cuda):
+    """64^4 native_xzwy with user buffers one element past a 16-byte boundary (the plane
+    kernels' and column kernels' staged paths)."""
+    torch = torch_cuda
+    dims = (64, 64, 64, 64)
+    f = F.ffts("float32", strategy_4d="native_xzwy").init(*dims)
+    x = O.random_4d(*dims, 23, layout=O.NATIVE_XZWY, single=True)
+    n = x.size
+    rb = torch.empty(n + 4, dtype=torch.float32, device="cuda")
+    xin = rb[1:1 + n].view(x.shape)
+    xin.copy_(_dev(torch, x))
+    sshape = f.spectrum_shape()
+    ns = int(np.prod(sshape))
+    sb = torch.empty(ns + 2, dtype=torch.complex64, device="cuda")
+    spec = sb[1:1 + ns].view(sshape)
+    ob = torch.empty(n + 4, dtype=torch.float32, device="cuda")
+    out = ob[1:1 + n].view(x.shape)
+    assert xin.data_ptr() % 16 and spec.data_ptr() % 16 and out.data_ptr() % 16
+    f.forward(xin, spec)
+    assert O.rel_l2(_host(spec), O.ffts4d_forward(O.NATIVE_XZWY, x, dims)) <= TOL
+    f.backward(spec, out, normalized=True)
+    assert O.rel_l2(_host(out), x) <= TOL
